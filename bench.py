@@ -1,0 +1,387 @@
+"""Benchmark: forward+backward ms per view of the differentiable Gaussian
+rasterizer on the batched training-step workload (1,000,000 Gaussians, SH
+degree 3, 8 views of 1280x720 per step, 0.8 L1 + 0.2 D-SSIM, fused Adam and
+densification statistics, CUDA-graph replay), next to the plain single-view
+path on the same scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own replica of the workload (the views of
+one step do not need another GPU); timings are the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd ms/view (1M Gaussians, 1280x720) batched vs plain; grad rel err"
+UNIT = "ms/view"
+WORKLOAD = "batched training step: 1,000,000 Gaussians, SH degree 3, 8 views of 1280x720 per step"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=1_000_000)
+    p.add_argument("--views", type=int, default=8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        try:
+            proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                     "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                    stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        while not self._stop.is_set():
+            line = proc.stdout.readline()
+            if not line:
+                break
+            self.rows.append([x.strip() for x in line.split(",")])
+        proc.terminate()
+        try:
+            proc.wait(timeout=5)
+        except Exception:
+            proc.kill()
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.3)
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_context(n, views, sh_dtype="f32"):
+    from rustscan_b200 import Context
+
+    return Context(max_splats=n, max_views=views, max_pixels=1280 * 720, max_isects=24 << 20, sh_dtype=sh_dtype)
+
+
+def fit_capacity(ctx, splats, cams):
+    """Render once; grow the intersection capacity if the scene needs more."""
+    from rustscan_b200 import GsrError
+
+    for _ in range(4):
+        try:
+            ctx.render_forward(splats, cams, check=True)
+            return
+        except GsrError as e:
+            if e.status != 3:
+                raise
+            ctx.reserve_isects(int(e.required * 1.15) + 1024)
+    raise RuntimeError("could not fit intersection capacity")
+
+
+def time_steps(fn, steps, warmup, world):
+    import torch
+
+    for i in range(warmup):
+        fn(i + 1)
+    torch.cuda.synchronize()
+    barrier(world)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for i in range(steps):
+        fn(warmup + i + 1)
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    return max_over_ranks(world, e0.elapsed_time(e1))
+
+
+def stage_profile(ctx, fn):
+    """Per-stage device times (ms) of one call of fn, from CUDA events on the launching stream."""
+    import torch
+
+    from rustscan_b200 import _lib
+
+    L = ctx._lib
+    L.gsr_profile(ctx._h, 1)
+    fn()
+    buf = (C.c_float * len(_lib.PROFILE_STAGES))()
+    ctx._check(L.gsr_profile_read(ctx._h, buf, len(_lib.PROFILE_STAGES),
+                                  C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    L.gsr_profile(ctx._h, 0)
+    return {k: float(buf[i]) for i, k in enumerate(_lib.PROFILE_STAGES)}
+
+
+def cpu_baseline(scene, cams, targets_np):
+    """Oracle (C++ restatement, OpenMP over all host threads) on one view of the workload."""
+    from oracle import oracle as O
+
+    cam = cams[0]
+    t0 = time.perf_counter()
+    f = O.Forward(scene.transforms, scene.sh, scene.raw_opacity, scene.sh_degree, cam)
+    _, vp = O.loss(f.image, targets_np[0])
+    f.backward(vp, mode=0)
+    dt = time.perf_counter() - t0
+    return {"value": dt * 1000.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": "1 of the 8 views (1M Gaussians, 1280x720): oracle forward + loss + exact backward, "
+                      "OpenMP over all host threads"}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle restatement of the reference's path on the host cores."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from rustscan_b200 import scenes as S
+
+    sc = S.config3(n=args.n, views=args.views)
+    gt = S.config3_targets(n=args.n)
+    gts = S.Scene(gt[0], gt[1], gt[2], 3, sc.cameras)
+    cams = sc.cameras
+    targets = {}
+
+    def step(i):
+        v = i % len(cams)
+        if v not in targets:
+            targets[v] = O.Forward(gts.transforms, gts.sh, gts.raw_opacity, 3, cams[v]).image[..., :3].copy()
+        f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, sc.sh_degree, cams[v])
+        _, vp = O.loss(f.image, targets[v])
+        f.backward(vp, mode=0)
+
+    for i in range(args.warmup):
+        step(i)
+    for i in range(args.warmup, args.warmup + args.steps):  # targets outside the timed region
+        v = i % len(cams)
+        if v not in targets:
+            targets[v] = O.Forward(gts.transforms, gts.sh, gts.raw_opacity, 3, cams[v]).image[..., :3].copy()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        step(i)
+    ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; see rustscan_b200/scenes.py)",
+            "config": {"workload": "one view per step of " + WORKLOAD, "n_gaussians": args.n,
+                       "resolution": "1280x720", "sh_degree": 3},
+            "cpu_baseline": {"value": ms, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": "one 1280x720 view per step: oracle forward + loss + exact backward"},
+            "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    from rustscan_b200 import LearningRates, Trainer, host_splats_to_device
+    from rustscan_b200 import scenes as S
+
+    world, rank, local = dist_setup(args)
+    sc = S.config3(seed_offset=rank, n=args.n, views=args.views)
+    gt_tr, gt_sh, gt_op = S.config3_targets(seed_offset=rank, n=args.n)
+    cams = sc.cameras
+    nv = len(cams)
+    H, W = cams[0].height, cams[0].width
+
+    # Targets: renders of the hidden ground-truth set.
+    ctx = make_context(args.n, nv)
+    gts = host_splats_to_device(S.Scene(gt_tr, gt_sh, gt_op, 3, cams))
+    fit_capacity(ctx, gts, cams)
+    flat, _, _ = ctx.render_forward(gts, cams)
+    targets = flat.view(nv, H, W, 4)[..., :3].contiguous()
+    del gts
+    splats = host_splats_to_device(sc)
+    fit_capacity(ctx, splats, cams)
+    counts = [ctx.export(v, "counts") for v in range(nv)]
+    V = [int(c[0]) for c in counts]
+    I = [int(c[1]) for c in counts]
+    P = H * W
+
+    # ---- batched, graph-replayed training step -----------------------------
+    trainer = Trainer(ctx, splats, LearningRates(), total_iterations=30000, use_graph=True)
+
+    def batched(it):
+        trainer.train_step(cams, targets, it)
+
+    for i in range(args.warmup):
+        batched(i + 1)
+    torch.cuda.synchronize()
+    ctx.sync_status()
+    with Clocks(local) as clk:
+        ms_total = time_steps(batched, args.steps, 0, world)
+    ms_step = ms_total / args.steps
+    value = ms_step / nv
+    kernels_per_step = int(ctx._lib.gsr_graph_kernel_count(ctx._h))
+
+    # ---- stage profile of one (non-graph) batched step: roofline ---------------
+    tr_prof = Trainer(ctx, splats, LearningRates(), use_graph=False)
+    tr_prof.opt = trainer.opt
+    stages = stage_profile(ctx, lambda: tr_prof.train_step(cams, targets, args.warmup + args.steps + 1))
+    hbm, peak_kind = peaks()
+    # Algorithmic bytes per launch (all views of the step).
+    algo = {
+        "raster_fwd": sum(40 * I[v] + 16 * P for v in range(nv)),
+        "raster_bwd": sum(40 * I[v] + 32 * P + 56 * V[v] for v in range(nv)),
+        "tile_sort": sum(24 * I[v] for v in range(nv)),
+        "project": 44 * args.n + sum((12 + 48 + 192) * V[v] for v in range(nv)),
+        "adam": 28 * (10 + 48 + 1) * args.n + 8 * 10 * args.n,
+    }
+    dom = max((k for k in algo), key=lambda k: stages.get(k, 0.0))
+    achieved = algo[dom] / (stages[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes": algo[dom], "launch_ms": stages[dom]}
+
+    # ---- plain single-view path (one view per call, FP32, no graph) ------------
+    plain = None
+    if not args.no_plain:
+        ctx1 = make_context(args.n, 1)
+        fit_capacity(ctx1, splats, [cams[0]])
+        tr1 = Trainer(ctx1, splats, LearningRates(), use_graph=False)
+
+        def plain_step(it):
+            v = (it - 1) % nv
+            tr1.train_step([cams[v]], targets[v], it)
+
+        ms1 = time_steps(plain_step, args.steps, args.warmup, world)
+        plain = ms1 / args.steps
+        ctx1.close()
+
+    # ---- end to end through the public API with host buffers -------------------
+    host_t = torch.empty(targets.shape, dtype=torch.float32, pin_memory=True)
+    host_t.copy_(targets.cpu())
+    dev_t = torch.empty_like(targets)
+    host_loss = torch.empty(nv, dtype=torch.float32, pin_memory=True)
+
+    def e2e_step(it):
+        dev_t.copy_(host_t, non_blocking=True)
+        loss = trainer.train_step(cams, dev_t, it)
+        host_loss.copy_(loss, non_blocking=True)
+
+    ms_e2e = time_steps(e2e_step, args.steps, 1, world) / args.steps
+    e2e = {"value": ms_e2e / nv, "unit": UNIT, "h2d_bytes_per_step": int(host_t.numel() * 4),
+           "d2h_bytes_per_step": int(nv * 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sc, cams, targets.cpu().numpy())
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; see rustscan_b200/scenes.py)",
+            "config": {"workload": WORKLOAD, "n_gaussians": args.n, "views_per_step": nv, "resolution": f"{W}x{H}",
+                       "sh_degree": 3, "sh_storage": "f32", "tile": "16x16", "loss": "0.8 L1 + 0.2 D-SSIM",
+                       "optimizer": "fused Adam (lr_pos 1.6e-4)", "graph": True,
+                       "l2": "inputs larger than L2 (params 236 MB + 8 views of state per step)",
+                       "visible_per_view": V, "intersections_per_view": I, "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "plain_single_view_ms_per_view": plain,
+            "stages_ms_per_step": stages,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": kernels_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+/* gsr.h — C ABI of the sm_100a differentiable Gaussian-splatting rasterizer.
+ *
+ * This is the drop-in boundary for RustGS's training render op. Each entry
+ * point names the reference interface it replaces (paths relative to the
+ * RustScan repository). A Rust backend binds these functions through a thin
+ * FFI crate; the reference's nine burn Backend extension traits collapse onto
+ * gsr_render_forward / gsr_render_backward plus the two primitives.
+ *
+ * Conventions
+ *  - All tensor arguments are device pointers (CUDA global memory) in the
+ *    RustGS layouts: transforms [N,10] f32 = position xyz + quaternion wxyz
+ *    + log-scale xyz; sh [N,K,3] (K = (degree+1)^2) f32 or bf16; raw
+ *    opacity [N] f32 logits (RustGS/src/training/engine/splats.rs:7-18).
+ *  - Images are [H,W,4] f32 RGBA, row-major, one view after another.
+ *  - Streams are cudaStream_t passed as void*. Calls only enqueue work; only
+ *    gsr_sync_status, gsr_export, gsr_profile_read and gsr_reserve_isects
+ *    synchronise the host, as their comments say.
+ *  - The caller owns every parameter, gradient and image buffer. The
+ *    context owns all scratch (keys, ranges, saved forward state).
+ *  - Errors are returned as gsr_status; nothing aborts or panics across the
+ *    ABI. gsr_last_error() gives a human-readable message.
+ *  - One context serves one stream at a time.
+ */
+#ifndef GSR_H
+#define GSR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GSR_API __attribute__((visibility("default")))
+#else
+#define GSR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gsr_status {
+  GSR_OK = 0,
+  GSR_ERR_INVALID_ARG = 1, /* bad pointer, size or configuration */
+  GSR_ERR_OOM = 2,         /* device allocation failed */
+  GSR_ERR_CAPACITY = 3,    /* intersection capacity exceeded; see gsr_sync_status */
+  GSR_ERR_CUDA = 4,        /* a CUDA call failed */
+  GSR_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  GSR_ERR_NOT_READY = 6    /* backward without a matching forward */
+} gsr_status;
+
+typedef struct gsr_ctx gsr_ctx;
+
+enum { GSR_SH_F32 = 0, GSR_SH_BF16 = 1 };
+enum { GSR_ADJOINT_EXACT = 0, GSR_ADJOINT_REFERENCE = 1 };
+
+/* Context configuration. Replaces the rasterizer fields of RustGS's
+ * TrainingConfig (RustGS/src/training/config.rs:7, raster_cov_blur) and the
+ * fixed TILE_WIDTH of RustGS/src/training/forward/mod.rs:25-26. Zero fields
+ * take the defaults noted. */
+typedef struct gsr_config {
+  float cov_blur;          /* screen-space covariance blur in px^2 (0.3) */
+  float background[3];     /* background colour (0,0,0) */
+  uint32_t tile_w, tile_h; /* tile shape: 16x16 (default), 8x8 or 32x8 */
+  uint32_t batch;          /* Gaussians staged in shared memory per batch (0: 256) */
+  int32_t sh_dtype;        /* GSR_SH_F32 or GSR_SH_BF16 storage of SH coefficients */
+  int32_t adjoint;         /* GSR_ADJOINT_EXACT (default) or GSR_ADJOINT_REFERENCE */
+  int32_t deterministic;   /* 1: fixed-order gradient reduction, bitwise reruns */
+  int32_t fp64_conic;      /* 1: 2x2 covariance inversion in FP64 */
+  uint64_t max_splats;     /* capacity in Gaussians */
+  uint32_t max_views;      /* views per forward (1) */
+  uint32_t _pad0;
+  uint64_t max_pixels;     /* capacity in pixels per view */
+  uint64_t max_isects;     /* tile intersections per view (0: 16 * max_splats, at least 2^20) */
+} gsr_config;
+
+/* Pinhole camera. viewmat is the column-major world->camera matrix
+ * (GaussianCamera::view_matrix, RustGS/src/core/camera.rs:30-32); campos is
+ * the world-space camera centre (GaussianCamera::position, :34-37). +Z is
+ * forward, +Y down, pixel centres at integer + 0.5. */
+typedef struct gsr_camera {
+  float viewmat[16];
+  float fx, fy, cx, cy;
+  uint32_t width, height;
+  float campos[3];
+  float _pad;
+} gsr_camera;
+
+/* Gaussian parameters (DeviceSplats, RustGS/src/training/engine/splats.rs:13-18). */
+typedef struct gsr_splats {
+  const float* transforms; /* [n,10] */
+  const void* sh;          /* [n,K,3] f32 or bf16 per gsr_config.sh_dtype */
+  const float* raw_opacity;/* [n] */
+  uint32_t n;
+  uint32_t sh_degree;      /* 0..4 */
+} gsr_splats;
+
+/* Gradients, same layouts as the parameters (f32). */
+typedef struct gsr_grads {
+  float* v_transforms;  /* [n,10] */
+  float* v_sh;          /* [n,K,3] */
+  float* v_raw_opacity; /* [n] */
+} gsr_grads;
+
+/* ---- context ------------------------------------------------------------ */
+GSR_API gsr_status gsr_create(const gsr_config* cfg, gsr_ctx** out);
+GSR_API void gsr_destroy(gsr_ctx* ctx);
+GSR_API const char* gsr_last_error(const gsr_ctx* ctx);
+GSR_API const char* gsr_version(void);
+
+/* Synchronises the stream, then reports device-side conditions of the work
+ * enqueued so far: GSR_ERR_CAPACITY with *required set to the intersection
+ * count that did not fit, GSR_ERR_TIMEOUT if a bounded wait gave up.
+ * Clears the conditions. Host-synchronising. */
+GSR_API gsr_status gsr_sync_status(gsr_ctx* ctx, void* stream, uint64_t* required);
+
+/* Grows the per-view intersection capacity (frees and reallocates scratch;
+ * call between steps). */
+GSR_API gsr_status gsr_reserve_isects(gsr_ctx* ctx, uint64_t max_isects);
+
+/* ---- primitives (RustGS/src/training/gpu_primitives) --------------------- */
+/* Inclusive scan of n u32 values.
+ * Replaces PrefixSumBackend::prefix_sum_u32_primitive
+ * (RustGS/src/training/gpu_primitives/prefix_sum.rs:41-45). in and out may
+ * not alias. n <= 2^30. */
+GSR_API gsr_status gsr_prefix_sum_u32(gsr_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t n, void* stream);
+
+/* Stable ascending sort of (key, value) pairs; equal keys keep input order.
+ * Replaces RadixSortBackend::radix_sort_by_key_u32_primitive
+ * (RustGS/src/training/gpu_primitives/radix_sort.rs:48-53). Inputs are not
+ * modified; outputs must not alias inputs. n <= 2^30. */
+GSR_API gsr_status gsr_radix_sort_by_key_u32(gsr_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
+                                     uint32_t* keys_out, uint32_t* vals_out, uint32_t n, void* stream);
+
+/* ---- render op ------------------------------------------------------------ */
+/* Forward render of n_views views: projection + SH, tile binning, depth and
+ * tile sorts, tile ranges and front-to-back blending, all enqueued without a
+ * host synchronisation. out_rgba receives the views' [H,W,4] images one
+ * after another; out_visible (nullable) receives [n_views, n] flags (1 if the
+ * Gaussian contributed to a pixel). The context keeps the state the backward
+ * needs until the next forward.
+ * Replaces render_forward (RustGS/src/training/forward/mod.rs:156-294) and,
+ * below it, ProjectionBackend (projection.rs:44-50), SortingBackend
+ * (sorting.rs:8-12), ProjectVisibleBackend (project_visible.rs:36-45),
+ * TileMappingBackend (tile_mapping.rs:82-95) and RasterizeBackend
+ * (rasterize.rs:48-59). */
+GSR_API gsr_status gsr_render_forward(gsr_ctx* ctx, const gsr_splats* splats, const gsr_camera* cams, uint32_t n_views,
+                              float* out_rgba, float* out_visible, void* stream);
+
+/* Backward of the last forward for upstream image gradients v_rgba (same
+ * layout as out_rgba). Writes the parameter gradients of the sum over views
+ * (rows of Gaussians no view sees are zero) and, if stats is not NULL, the
+ * [n_views, n, 7] densification statistics (project_backwards.wgsl:192-277).
+ * Replaces RenderBackward::backward (RustGS/src/training/backward/autodiff.rs:82-142)
+ * and, below it, RasterizeBwdBackend (rasterize_bwd.rs:41-54) and
+ * ProjectBwdBackend (project_bwd.rs:44-52). */
+GSR_API gsr_status gsr_render_backward(gsr_ctx* ctx, const gsr_splats* splats, const float* v_rgba, const gsr_grads* grads,
+                               float* stats, void* stream);
+
+/* Copies internal state of view `view` of the last forward to a device or
+ * host buffer for inspection (tests, tools). `what` selects:
+ *  0 counts (u32 x2: visible, intersections)          [host-synchronising]
+ *  1 visible global ids in compact order (u32 x V)
+ *  2 depth order: compact index per rank (u32 x V)
+ *  3 sorted intersection tile ids (u32 x I)
+ *  4 sorted intersection compact indices (u32 x I)
+ *  5 tile ranges (u32 x 2T)
+ *  6 per-pixel final transmittance (f32 x H*W)
+ *  7 per-pixel last contributor list index + 1 (u32 x H*W, 0: none)
+ *  8 per-pixel contributor counts (u32 x H*W)
+ *  9 per-Gaussian screen-space gradient sums of the last backward (f32 x 12V)
+ * 10 per-pixel list entries evaluated (u32 x H*W)
+ * 11 per-Gaussian tile counts in compact order (u32 x V)
+ * `bytes` is the destination size; the call fails if it is too small. */
+GSR_API gsr_status gsr_export(gsr_ctx* ctx, uint32_t view, int32_t what, void* dst, uint64_t bytes, void* stream);
+
+/* ---- loss (RustGS/src/training/engine/loss.rs:112-142) -------------------- */
+/* l1_w * mean|pred - target| + ssim_w * (1 - mean SSIM) with an 11-tap
+ * sigma-1.5 Gaussian window, replicate padding and C1 = 0.01^2,
+ * C2 = 0.03^2, for n_views images. pred is RGBA [H,W,4] per view (the render
+ * output), target RGB [H,W,3] per view. Writes loss[n_views] and the
+ * gradient v_pred in RGBA layout (alpha gradient 0). Replaces
+ * combined_loss_with_kernel and its burn autodiff backward with the default
+ * (non-robust, unmasked) settings. */
+GSR_API gsr_status gsr_loss(gsr_ctx* ctx, const float* pred, const float* target, const gsr_camera* cams, uint32_t n_views,
+                    float l1_w, float ssim_w, float* loss, float* v_pred, void* stream);
+
+/* ---- optimizer (RustGS/src/training/engine/optimizer.rs:45-163) ----------- */
+typedef struct gsr_adam_state {
+  float* m_transforms; float* v_transforms; /* [n,10] */
+  float* m_sh; float* v_sh;                 /* [n,K,3] */
+  float* m_opacity; float* v_opacity;       /* [n] */
+} gsr_adam_state;
+
+typedef struct gsr_lr {
+  float position, rotation, scale, color, opacity; /* learning rates per column group */
+  float beta1, beta2, eps;                         /* 0.9, 0.999, 1e-8 */
+} gsr_lr;
+
+/* Bias-corrected Adam with per-column learning rates on all three parameter
+ * groups; step is the 1-based step count shared by the groups.
+ * Parameters are updated in place (the SH storage dtype is honoured).
+ * Replaces AdamScaled::step_device_splats (optimizer.rs:80-120). */
+GSR_API gsr_status gsr_adam_step(gsr_ctx* ctx, float* transforms, void* sh, float* raw_opacity, uint32_t n,
+                         uint32_t sh_degree, const gsr_grads* grads, const gsr_adam_state* state, const gsr_lr* lr,
+                         int32_t step, void* stream);
+
+/* ---- densification statistics (RustGS/src/training/engine/trainer.rs:651-728) */
+/* acc holds 9 arrays of n floats: grad_2d, screen_grad_2d, abs_grad_2d,
+ * abs_pixel_grad_2d, pixel_coverage, camera_depth, grad_color,
+ * num_observations, visible_observations. visible may be NULL when
+ * use_visible is 0. Replaces WgpuTrainer::accumulate_gradients. */
+GSR_API gsr_status gsr_accumulate_densify(gsr_ctx* ctx, const gsr_grads* grads, const float* stats, const float* visible,
+                                  uint32_t n, uint32_t sh_degree, int32_t use_visible, float* acc, void* stream);
+
+/* ---- training step (RustGS/src/training/engine/trainer.rs:253-440) ------- */
+typedef struct gsr_train_params {
+  gsr_lr lr;
+  int32_t step;        /* 1-based Adam step */
+  float l1_weight;     /* 0.8 */
+  float ssim_weight;   /* 0.2 */
+  int32_t use_visible; /* densification visible_observations from render visibility */
+} gsr_train_params;
+
+/* One training step over n_views views: forward, loss, backward, the
+ * densification accumulators (per view) and one fused Adam update of all
+ * parameters with the gradient of the mean loss over the views. targets are
+ * RGB [H,W,3] per view on the device; loss[n_views] receives the per-view
+ * losses (device). With use_graph != 0 the step is recorded into a CUDA graph
+ * on first use for this (splats, cameras, sizes) signature and replayed
+ * afterwards. */
+GSR_API gsr_status gsr_train_step(gsr_ctx* ctx, float* transforms, void* sh, float* raw_opacity, uint32_t n,
+                          uint32_t sh_degree, const gsr_adam_state* state, const gsr_camera* cams, uint32_t n_views,
+                          const float* targets, const gsr_train_params* params, float* densify_acc, float* loss,
+                          int32_t use_graph, void* stream);
+
+/* ---- instrumentation (no counterpart in the reference) ------------------ */
+/* Stage timing: when enabled, the context records CUDA events on the stream
+ * between pipeline stages of the calls that follow (never inside a graph
+ * capture). gsr_profile_read synchronises the stream and writes the
+ * milliseconds per stage, summed since the last read, in this order:
+ * project, depth_sort, offsets, emit, tile_sort, ranges, raster_fwd,
+ * visible, loss, raster_bwd, reduce, project_bwd, adam (13 entries). */
+enum { GSR_PROFILE_STAGES = 13 };
+GSR_API gsr_status gsr_profile(gsr_ctx* ctx, int32_t enable);
+GSR_API gsr_status gsr_profile_read(gsr_ctx* ctx, float* ms_per_stage, int32_t n_stages, void* stream);
+/* Kernel nodes in the captured training-step graph (0 before a capture). */
+GSR_API int32_t gsr_graph_kernel_count(const gsr_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSR_H */

@@ -1,0 +1,400 @@
+"""rustscan_b200 — B200-native differentiable Gaussian-splatting rasterizer.
+
+A host-side mirror of RustGS's renderer/trainer API over the C ABI of
+``libgsr.so`` (include/gsr.h). PyTorch supplies device memory and streams;
+all computation happens in the library's sm_100a kernels.
+
+Reference interfaces mirrored here:
+  * ``DeviceSplats``             — RustGS/src/training/engine/splats.rs:13-63
+  * ``render_forward``           — RustGS/src/training/forward/mod.rs:156-294
+  * ``render_splats_with_visibility`` (autograd op with ``RenderBackward``)
+                                 — RustGS/src/training/backward/autodiff.rs:82-251
+  * ``prefix_sum_u32`` / ``radix_sort_by_key_u32``
+                                 — RustGS/src/training/gpu_primitives/*.rs
+  * ``combined_loss``            — RustGS/src/training/engine/loss.rs:112-142
+  * ``AdamScaled``               — RustGS/src/training/engine/optimizer.rs:45-163
+  * ``Trainer.train_step``       — RustGS/src/training/engine/trainer.rs:253-440
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import GsrError
+from .scenes import Camera, Scene  # noqa: F401  (re-exported)
+
+DEFAULT_RASTER_COV_BLUR = 0.3  # RustGS/src/training/config.rs:7
+
+EXPORT = dict(counts=0, gids=1, depth_order=2, isect_tiles=3, isect_vals=4, tile_ranges=5, tfinal=6, last=7,
+              ncontrib=8, splat_grads=9, nvisit=10, tile_counts=11)
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("rustscan_b200 needs a CUDA device (sm_100a); none is available")
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def camera_struct(cam: Camera) -> _lib.gsr_camera:
+    c = _lib.gsr_camera()
+    for i in range(16):
+        c.viewmat[i] = float(cam.viewmat[i])
+    c.fx, c.fy, c.cx, c.cy = float(cam.fx), float(cam.fy), float(cam.cx), float(cam.cy)
+    c.width, c.height = int(cam.width), int(cam.height)
+    for i in range(3):
+        c.campos[i] = float(cam.campos[i])
+    return c
+
+
+def camera_array(cams):
+    arr = (_lib.gsr_camera * len(cams))()
+    for i, cam in enumerate(cams):
+        arr[i] = camera_struct(cam)
+    return arr
+
+
+@dataclasses.dataclass
+class DeviceSplats:
+    """GPU-resident Gaussians in the RustGS packed layout."""
+
+    transforms: torch.Tensor  # [N,10] f32
+    sh_coeffs: torch.Tensor  # [N,K,3] f32 or bf16
+    raw_opacities: torch.Tensor  # [N] f32
+    sh_degree: int
+
+    def num_splats(self) -> int:
+        return int(self.transforms.shape[0])
+
+    def struct(self) -> _lib.gsr_splats:
+        s = _lib.gsr_splats()
+        s.transforms = self.transforms.data_ptr()
+        s.sh = self.sh_coeffs.data_ptr()
+        s.raw_opacity = self.raw_opacities.data_ptr()
+        s.n = self.num_splats()
+        s.sh_degree = int(self.sh_degree)
+        return s
+
+
+def host_splats_to_device(scene, device="cuda", sh_dtype=torch.float32) -> DeviceSplats:
+    """engine/splats.rs:26-63: upload a host scene."""
+    return DeviceSplats(
+        torch.as_tensor(np.ascontiguousarray(scene.transforms), device=device),
+        torch.as_tensor(np.ascontiguousarray(scene.sh), device=device).to(sh_dtype).contiguous(),
+        torch.as_tensor(np.ascontiguousarray(scene.raw_opacity), device=device),
+        int(scene.sh_degree),
+    )
+
+
+class Context:
+    """Owns the library context (scratch, saved forward state) for one stream."""
+
+    def __init__(self, max_splats, max_views=1, max_pixels=1920 * 1080, max_isects=0, tile=(16, 16),
+                 sh_dtype="f32", adjoint="exact", deterministic=False, fp64_conic=False,
+                 cov_blur=DEFAULT_RASTER_COV_BLUR, background=(0.0, 0.0, 0.0), batch=0):
+        _require_cuda()
+        self._lib = _lib.load()
+        cfg = _lib.gsr_config()
+        cfg.cov_blur = float(cov_blur)
+        for i in range(3):
+            cfg.background[i] = float(background[i])
+        cfg.tile_w, cfg.tile_h = int(tile[0]), int(tile[1])
+        cfg.batch = int(batch)
+        cfg.sh_dtype = _lib.GSR_SH_BF16 if sh_dtype in ("bf16", torch.bfloat16) else _lib.GSR_SH_F32
+        cfg.adjoint = _lib.GSR_ADJOINT_REFERENCE if adjoint == "reference" else _lib.GSR_ADJOINT_EXACT
+        cfg.deterministic = int(bool(deterministic))
+        cfg.fp64_conic = int(bool(fp64_conic))
+        cfg.max_splats = int(max_splats)
+        cfg.max_views = int(max_views)
+        cfg.max_pixels = int(max_pixels)
+        cfg.max_isects = int(max_isects)
+        self.cfg = cfg
+        self.background = tuple(float(b) for b in background)
+        h = C.c_void_p()
+        torch.cuda.init()
+        st = self._lib.gsr_create(C.byref(cfg), C.byref(h))
+        if st != _lib.GSR_OK:
+            raise GsrError(st, "gsr_create failed")
+        self._h = h
+        self._fwd_cams = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gsr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != _lib.GSR_OK:
+            raise GsrError(st, self._lib.gsr_last_error(self._h).decode())
+
+    # ---- status ------------------------------------------------------------
+    def sync_status(self):
+        """Synchronise and raise GsrError on capacity overflow or timeout."""
+        req = C.c_uint64(0)
+        st = self._lib.gsr_sync_status(self._h, _stream(), C.byref(req))
+        if st != _lib.GSR_OK:
+            err = GsrError(st, self._lib.gsr_last_error(self._h).decode())
+            err.required = int(req.value)
+            raise err
+
+    def reserve_isects(self, n):
+        self._check(self._lib.gsr_reserve_isects(self._h, int(n)))
+
+    # ---- primitives ----------------------------------------------------------
+    def prefix_sum_u32(self, x: torch.Tensor) -> torch.Tensor:
+        """Inclusive scan (PrefixSumBackend::prefix_sum_u32_primitive)."""
+        x = x.contiguous()
+        out = torch.empty_like(x)
+        if x.numel():
+            self._check(self._lib.gsr_prefix_sum_u32(self._h, _ptr(x), _ptr(out), x.numel(), _stream()))
+        return out
+
+    def radix_sort_by_key_u32(self, keys: torch.Tensor, vals: torch.Tensor):
+        """Stable sort of (key, value) pairs (RadixSortBackend::radix_sort_by_key_u32_primitive)."""
+        keys = keys.contiguous()
+        vals = vals.contiguous()
+        ko = torch.empty_like(keys)
+        vo = torch.empty_like(vals)
+        if keys.numel():
+            self._check(self._lib.gsr_radix_sort_by_key_u32(self._h, _ptr(keys), _ptr(vals), _ptr(ko), _ptr(vo),
+                                                            keys.numel(), _stream()))
+        return ko, vo
+
+    # ---- render op -------------------------------------------------------------
+    def render_forward(self, splats: DeviceSplats, cameras, visible=False, check=True):
+        """Render views; returns (images [list of H,W,4 views of one buffer], visible [V,N] or None)."""
+        cams = list(cameras)
+        total = sum(c.width * c.height for c in cams)
+        out = torch.empty(total * 4, dtype=torch.float32, device="cuda")
+        vis = torch.empty((len(cams), splats.num_splats()), dtype=torch.float32, device="cuda") if visible else None
+        s = splats.struct()
+        arr = camera_array(cams)
+        self._check(self._lib.gsr_render_forward(self._h, C.byref(s), arr, len(cams), _ptr(out), _ptr(vis),
+                                                 _stream()))
+        if check:
+            self.sync_status()
+        self._fwd_cams = cams
+        imgs, o = [], 0
+        for c in cams:
+            n = c.width * c.height * 4
+            imgs.append(out[o:o + n].view(c.height, c.width, 4))
+            o += n
+        return out, imgs, vis
+
+    def render_backward(self, splats: DeviceSplats, v_rgba: torch.Tensor, stats=True):
+        """Parameter gradients of the last forward for upstream image gradients."""
+        n = splats.num_splats()
+        K = (splats.sh_degree + 1) ** 2
+        g = dict(
+            v_transforms=torch.empty((n, 10), dtype=torch.float32, device="cuda"),
+            v_sh=torch.empty((n, K, 3), dtype=torch.float32, device="cuda"),
+            v_raw_opacity=torch.empty(n, dtype=torch.float32, device="cuda"),
+        )
+        nv = len(self._fwd_cams) if self._fwd_cams else 1
+        g["stats"] = torch.empty((nv, n, 7), dtype=torch.float32, device="cuda") if stats else None
+        gs = _lib.gsr_grads(g["v_transforms"].data_ptr(), g["v_sh"].data_ptr(), g["v_raw_opacity"].data_ptr())
+        s = splats.struct()
+        v = v_rgba.contiguous()
+        self._check(self._lib.gsr_render_backward(self._h, C.byref(s), _ptr(v), C.byref(gs), _ptr(g["stats"]),
+                                                  _stream()))
+        return g
+
+    def export(self, view, what):
+        """Copy internal state of the last forward to the host (numpy)."""
+        code = EXPORT[what] if isinstance(what, str) else int(what)
+        cnt = np.zeros(2, np.uint32)
+        self._check(self._lib.gsr_export(self._h, view, 0, cnt.ctypes.data, 8, _stream()))
+        V, I = int(cnt[0]), int(cnt[1])
+        cam = self._fwd_cams[view]
+        P = cam.width * cam.height
+        tx = math.ceil(cam.width / self.cfg.tile_w)
+        ty = math.ceil(cam.height / self.cfg.tile_h)
+        shapes = {0: (2, np.uint32), 1: (V, np.uint32), 2: (V, np.uint32), 3: (I, np.uint32), 4: (I, np.uint32),
+                  5: (2 * tx * ty, np.uint32), 6: (P, np.float32), 7: (P, np.uint32), 8: (P, np.uint32),
+                  9: (12 * V, np.float32), 10: (P, np.uint32), 11: (V, np.uint32)}
+        if code == 0:
+            return cnt
+        n, dt = shapes[code]
+        out = np.zeros(max(n, 1), dt)
+        self._check(self._lib.gsr_export(self._h, view, code, out.ctypes.data, out.nbytes, _stream()))
+        return out[:n]
+
+    # ---- loss / optimizer ----------------------------------------------------------
+    def loss(self, pred: torch.Tensor, target: torch.Tensor, cameras, l1_weight=0.8, ssim_weight=0.2):
+        """combined_loss_with_kernel: per-view loss values and d loss / d pred (RGBA layout)."""
+        cams = list(cameras)
+        loss = torch.empty(len(cams), dtype=torch.float32, device="cuda")
+        vp = torch.empty_like(pred)
+        arr = camera_array(cams)
+        self._check(self._lib.gsr_loss(self._h, _ptr(pred.contiguous()), _ptr(target.contiguous()), arr, len(cams),
+                                       float(l1_weight), float(ssim_weight), _ptr(loss), _ptr(vp), _stream()))
+        return loss, vp
+
+
+def prefix_sum_u32(x: torch.Tensor, ctx: Context | None = None) -> torch.Tensor:
+    ctx = ctx or Context(max_splats=max(x.numel(), 1))
+    return ctx.prefix_sum_u32(x)
+
+
+def radix_sort_by_key_u32(keys: torch.Tensor, vals: torch.Tensor, ctx: Context | None = None):
+    ctx = ctx or Context(max_splats=max(keys.numel(), 1))
+    return ctx.radix_sort_by_key_u32(keys, vals)
+
+
+def render_forward(ctx: Context, splats: DeviceSplats, camera: Camera, visible=True):
+    """forward/mod.rs:156-294 for one view: (image [H,W,4], visible [N])."""
+    _, imgs, vis = ctx.render_forward(splats, [camera], visible=visible)
+    return imgs[0], (vis[0] if vis is not None else None)
+
+
+class _RenderFn(torch.autograd.Function):
+    """The render op with RenderBackward (backward/autodiff.rs:82-142) as its backward."""
+
+    @staticmethod
+    def forward(fctx, ctx, splats, camera, transforms, sh, raw_opacity, stats_leaf):
+        img, vis = render_forward(ctx, splats, camera, visible=True)
+        fctx.ctx = ctx
+        fctx.splats = splats
+        fctx.mark_non_differentiable(vis)
+        return img.clone(), vis
+
+    @staticmethod
+    def backward(fctx, v_img, _v_vis):
+        g = fctx.ctx.render_backward(fctx.splats, v_img.contiguous(), stats=True)
+        return (None, None, None, g["v_transforms"], g["v_sh"], g["v_raw_opacity"], g["stats"][0])
+
+
+@dataclasses.dataclass
+class RenderSplatsOutput:
+    image: torch.Tensor
+    visible: torch.Tensor
+    screen_grad_stats: torch.Tensor
+
+
+def render_splats_with_visibility(ctx: Context, splats: DeviceSplats, camera: Camera) -> RenderSplatsOutput:
+    """backward/autodiff.rs:240-251: differentiable render; the [N,7] densification
+    statistics arrive as the gradient of ``screen_grad_stats`` (autodiff.rs:192-194)."""
+    stats_leaf = torch.zeros((splats.num_splats(), 7), device="cuda", requires_grad=True)
+    img, vis = _RenderFn.apply(ctx, splats, camera, splats.transforms, splats.sh_coeffs, splats.raw_opacities,
+                               stats_leaf)
+    return RenderSplatsOutput(img, vis, stats_leaf)
+
+
+@dataclasses.dataclass
+class LearningRates:
+    """TrainingOptimizerConfig defaults (RustGS/src/training/config.rs:532-546)."""
+
+    position: float = 0.00016
+    position_final: float = 0.0000016
+    rotation: float = 0.001
+    scale: float = 0.005
+    color: float = 0.0025
+    opacity: float = 0.05
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+
+    def at(self, iteration, total):
+        """Exponential position decay (engine/trainer.rs:179-195); the others stay constant."""
+        pos = self.position
+        if 0 < self.position_final < self.position and total > 0:
+            t = min(iteration, total) / total
+            pos = self.position * math.exp(math.log(self.position_final / self.position) * t)
+        lr = _lib.gsr_lr()
+        lr.position, lr.rotation, lr.scale, lr.color, lr.opacity = pos, self.rotation, self.scale, self.color, self.opacity
+        lr.beta1, lr.beta2, lr.eps = self.beta1, self.beta2, self.eps
+        return lr
+
+
+class AdamScaled:
+    """Bias-corrected Adam with per-column learning rates (engine/optimizer.rs:45-163)."""
+
+    def __init__(self, ctx: Context, splats: DeviceSplats, lrs: LearningRates | None = None):
+        self.ctx = ctx
+        self.lrs = lrs or LearningRates()
+        n, K = splats.num_splats(), (splats.sh_degree + 1) ** 2
+        z = lambda *s: torch.zeros(s, dtype=torch.float32, device="cuda")  # noqa: E731
+        self.m_tr, self.v_tr = z(n, 10), z(n, 10)
+        self.m_sh, self.v_sh = z(n, K, 3), z(n, K, 3)
+        self.m_op, self.v_op = z(n), z(n)
+        self.step = 0
+
+    def state(self):
+        return _lib.gsr_adam_state(self.m_tr.data_ptr(), self.v_tr.data_ptr(), self.m_sh.data_ptr(),
+                                   self.v_sh.data_ptr(), self.m_op.data_ptr(), self.v_op.data_ptr())
+
+    def reset(self):
+        for t in (self.m_tr, self.v_tr, self.m_sh, self.v_sh, self.m_op, self.v_op):
+            t.zero_()
+        self.step = 0
+
+    def step_device_splats(self, splats: DeviceSplats, grads: dict, lr: _lib.gsr_lr | None = None):
+        self.step += 1
+        lr = lr or self.lrs.at(0, 0)
+        gs = _lib.gsr_grads(grads["v_transforms"].data_ptr(), grads["v_sh"].data_ptr(),
+                            grads["v_raw_opacity"].data_ptr())
+        st = self.state()
+        self.ctx._check(self.ctx._lib.gsr_adam_step(
+            self.ctx._h, _ptr(splats.transforms), _ptr(splats.sh_coeffs), _ptr(splats.raw_opacities),
+            splats.num_splats(), splats.sh_degree, C.byref(gs), C.byref(st), C.byref(lr), self.step, _stream()))
+
+
+class Trainer:
+    """The device part of WgpuTrainer::train_step (engine/trainer.rs:253-440):
+    render all views, 0.8 L1 + 0.2 D-SSIM, backward, densification statistics
+    (engine/trainer.rs:651-728) and one fused Adam update, optionally replayed
+    from a CUDA graph."""
+
+    ACC_NAMES = ("grad_2d", "screen_grad_2d", "abs_grad_2d", "abs_pixel_grad_2d", "pixel_coverage", "camera_depth",
+                 "grad_color", "num_observations", "visible_observations")
+
+    def __init__(self, ctx: Context, splats: DeviceSplats, lrs: LearningRates | None = None, total_iterations=30000,
+                 l1_weight=0.8, ssim_weight=0.2, use_visible=False, use_graph=True):
+        self.ctx = ctx
+        self.splats = splats
+        self.opt = AdamScaled(ctx, splats, lrs)
+        self.total = total_iterations
+        self.l1_weight, self.ssim_weight = l1_weight, ssim_weight
+        self.use_visible = use_visible
+        self.use_graph = use_graph
+        self.densify = torch.zeros((9, splats.num_splats()), dtype=torch.float32, device="cuda")
+        self.loss = None
+        self._cams = None
+
+    def train_step(self, cameras, targets: torch.Tensor, iteration: int):
+        cams = list(cameras)
+        if self.loss is None or self.loss.numel() != len(cams):
+            self.loss = torch.zeros(len(cams), dtype=torch.float32, device="cuda")
+        self.opt.step += 1
+        p = _lib.gsr_train_params()
+        p.lr = self.opt.lrs.at(max(iteration - 1, 0), self.total)
+        p.step = self.opt.step
+        p.l1_weight, p.ssim_weight = self.l1_weight, self.ssim_weight
+        p.use_visible = int(self.use_visible)
+        if self._cams is not cams:
+            self._arr = camera_array(cams)
+            self._cams = cams
+        st = self.opt.state()
+        s = self.splats
+        self.ctx._check(self.ctx._lib.gsr_train_step(
+            self.ctx._h, _ptr(s.transforms), _ptr(s.sh_coeffs), _ptr(s.raw_opacities), s.num_splats(), s.sh_degree,
+            C.byref(st), self._arr, len(cams), _ptr(targets), C.byref(p), _ptr(self.densify), _ptr(self.loss),
+            int(self.use_graph), _stream()))
+        return self.loss

@@ -1,0 +1,166 @@
+// gsr_kernels.h — host-side launchers of the rasterizer kernels and the
+// device buffer layout they share. Internal to libgsr.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gsr_internal.cuh"
+
+namespace gsr {
+
+constexpr int kMaxViews = kMaxSegments;
+
+// Per-view scratch of one forward/backward. Every array is sized for
+// max_views slots; view v's slice starts at v * <capacity>.
+struct FwdBufs {
+  float4* rec;             // [V][3] projected record (see k_project.cu)
+  uint32_t* gid_of_c;      // [V] global id of compact index c (global-id order)
+  uint32_t* depth_key;     // [V] f32 depth bits of c
+  uint32_t* perm;          // [V] compact index of depth rank r
+  uint32_t* depth_sorted;  // [V] sorted depth keys (sort output, unused after)
+  uint32_t* key_tmp;       // [max(V, I)] sort double buffers
+  uint32_t* val_tmp;
+  uint32_t* count;         // [V] tile count of c
+  uint32_t* offset;        // [V] first intersection of rank r
+  int32_t* c_of_gid;       // [N] compact index of a global id, -1 if culled
+  uint32_t* isect_key;     // [I] tile id, sorted
+  uint32_t* isect_val;     // [I] compact index, sorted
+  uint32_t* isect_key_raw; // [I] emission order
+  uint32_t* isect_val_raw;
+  uint32_t* ranges;        // [2T]
+  float* tfinal;           // [P] final transmittance
+  uint32_t* last;          // [P] last contributor list index + 1
+  uint32_t* ncontrib;      // [P]
+  uint32_t* nvisit;        // [P]
+  uint8_t* visible_c;      // [V]
+  float4* sgrad;           // [V][3] screen-space gradient sums (12 floats)
+  float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)
+  uint32_t* inv_perm;      // [I] emission index -> sorted position (deterministic mode)
+  uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
+  uint64_t Vcap, Ncap, Icap, Tcap, Pcap;
+};
+
+struct ViewSet {
+  const ViewDesc* views;  // device
+  uint32_t n_views;
+  uint32_t tile_w, tile_h;
+  uint32_t total_tiles;   // sum over views of tiles_x * tiles_y
+  uint32_t max_tiles;     // max over views
+};
+
+struct SplatsDev {
+  const float* transforms;
+  const void* sh;
+  const float* raw_opac;
+  uint32_t n;
+  int degree;
+  int sh_bf16;
+};
+
+// Pointers to a view's slice of a per-view array.
+template <class T> __host__ __device__ __forceinline__ T* slice(T* base, uint64_t cap, uint32_t v) {
+  return base + (size_t)cap * v;
+}
+
+struct Scratch {
+  unsigned long long* lb_states;  // look-back states
+  uint64_t lb_states_words;
+  uint32_t* hist;                 // radix histograms [segments][4][256]
+  uint32_t* hist_base;            // their exclusive scans
+  LookbackCtl* ctl;
+  DevStatus* status;
+  int num_sms;
+};
+
+// ---- launchers (return cudaGetLastError()) ----
+cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blur, int fp64_conic, FwdBufs& b,
+                           const Scratch& s, cudaStream_t st);
+
+// Stable LSD radix sort of (key, value) pairs in `segments` segments of
+// seg_stride elements; segment i holds counts[i * count_stride] elements
+// (or n_host when counts is null). vals_in == nullptr means values 0..n-1.
+// The result lands in keys_out/vals_out; tmp buffers are clobbered.
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                             uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
+                             uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
+                             uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st);
+
+// Inclusive scan of n_host values (prefix sum primitive).
+cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_host, const Scratch& s,
+                               cudaStream_t st);
+
+// Per view: offset[r] = exclusive scan of count[perm[r]], sets vcount[1..2].
+cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+
+cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
+cudaError_t launch_remap(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+cudaError_t launch_ranges(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+
+cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, float* out_rgba, const Scratch& s,
+                              cudaStream_t st);
+cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, const float* v_rgba, int ref_mode,
+                              int deterministic, const Scratch& s, cudaStream_t st);
+cudaError_t launch_reduce_det(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+
+// Copies view descriptors to device memory through a kernel argument (safe
+// to enqueue repeatedly and to capture in a graph).
+struct ViewDescBlock {
+  ViewDesc v[kMaxViews];
+};
+cudaError_t launch_set_views(ViewDesc* dst, const ViewDesc* host, uint32_t n, cudaStream_t st);
+
+cudaError_t launch_visible_out(const ViewSet& vs, FwdBufs& b, uint32_t n, float* out_visible, cudaStream_t st);
+
+// Per-step optimizer scalars, read by the kernels from device memory so that
+// a captured step can be replayed with new values.
+struct AdamScalars {
+  float lr_pos, lr_rot, lr_scale, lr_color, lr_opac;
+  float beta1, beta2, eps, bc1, bc2;
+};
+
+struct AdamArgs {
+  float* transforms;
+  void* sh;
+  float* raw_opac;
+  float* m_tr;
+  float* v_tr;
+  float* m_sh;
+  float* v_sh;
+  float* m_op;
+  float* v_op;
+  const AdamScalars* scal;  // device
+};
+
+// Writes the scalars to device memory (a one-thread kernel, so the values
+// travel as launch arguments and the call is safe to issue per step).
+cudaError_t launch_set_scalars(AdamScalars* dst, const AdamScalars& v, cudaStream_t st);
+
+// Project backward over all Gaussians for all views of the last forward.
+// mode 0 writes gradients (grad_* non-null, summed over views, scaled by
+// grad_scale) and optional per-view stats; mode 1 applies Adam in place
+// (adam non-null) and accumulates the densification statistics.
+struct ProjBwdArgs {
+  float* v_tr;
+  float* v_sh;
+  float* v_op;
+  float* stats;  // [views][n][7] or null
+  const AdamArgs* adam;
+  float* densify_acc;  // [9][n] or null
+  int use_visible;
+  float grad_scale;
+  int exact;
+};
+cudaError_t launch_project_bwd(const SplatsDev& sp, const ViewSet& vs, float cov_blur, FwdBufs& b,
+                               const ProjBwdArgs& a, const AdamArgs* adam, cudaStream_t st, int num_sms);
+
+cudaError_t launch_adam(const AdamArgs& a, const float* g_tr, const float* g_sh, const float* g_op, uint32_t n,
+                        int degree, int sh_bf16, cudaStream_t st, int num_sms);
+cudaError_t launch_densify(const float* v_tr, const float* stats, const float* v_sh, const float* visible, uint32_t n,
+                           int degree, int use_visible, float* acc, cudaStream_t st, int num_sms);
+
+// Loss: per view, l1_w*L1 + ssim_w*(1-SSIM); writes loss[v] and v_pred (RGBA).
+cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const float* pred, const float* target,
+                        float l1_w, float ssim_w, float* loss, float* v_pred, float* work, uint64_t work_floats,
+                        cudaStream_t st);
+
+}  // namespace gsr

@@ -287,6 +287,38 @@ template <class F> GSR_HD V3<F> inverse2x2_packed(const M2<F>& m) {
   return o;
 }
 
+// FP64 variants of the compensation and the inversion for float inputs,
+// used for near-degenerate (flattened) covariances where the float
+// determinant a*d - b*c cancels catastrophically. The float matrix is
+// widened, the determinants and the inverse are formed in double, and the
+// results are rounded once to float. For double inputs they are the plain
+// functions.
+GSR_HD float compensate_cov2d_hp(M2<float>& cov, float blur) {
+  const double a = cov.m[0][0], b = cov.m[0][1], c = cov.m[1][0], d = cov.m[1][1];
+  cov.m[0][0] = cov.m[0][0] + blur;
+  cov.m[1][1] = cov.m[1][1] + blur;
+  const double det_raw = fmax(a * d - b * c, 0.0);
+  const double det_end = fmax((double)cov.m[0][0] * (double)cov.m[1][1] - b * c, 1e-12);
+  if (det_raw <= 0.0) return 0.0f;
+  return (float)sqrt(det_raw / det_end);
+}
+GSR_HD double compensate_cov2d_hp(M2<double>& cov, double blur) { return compensate_cov2d(cov, blur); }
+GSR_HD V3<float> inverse2x2_packed_hp(const M2<float>& m) {
+  const double a = (double)m.m[0][0] + 1e-6, d = (double)m.m[1][1] + 1e-6, b = m.m[0][1];
+  const double det = a * d - b * (double)m.m[1][0];
+  V3<float> o;
+  if (det <= 1e-10) {
+    o.x = o.y = o.z = 0.0f;
+    return o;
+  }
+  const double inv = 1.0 / det;
+  o.x = (float)(d * inv);
+  o.y = (float)(-b * inv);
+  o.z = (float)(a * inv);
+  return o;
+}
+GSR_HD V3<double> inverse2x2_packed_hp(const M2<double>& m) { return inverse2x2_packed(m); }
+
 // helpers.wgsl:218-224.
 template <class F> GSR_HD V2<F> bbox_extent(const M2<F>& cov, F thr) {
   const F sp = gmax(thr, F(0));
@@ -507,7 +539,8 @@ template <class F> struct Projected {
 // reciprocal square root of its squared norm (project_forward.wgsl:38-42).
 template <class F>
 GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, V3<F> log_scale, F raw_opac,
-                                     F cov_blur, TileShape ts, uint32_t tiles_x, uint32_t tiles_y) {
+                                     F cov_blur, TileShape ts, uint32_t tiles_x, uint32_t tiles_y,
+                                     bool hp = false) {
   Projected<F> p;
   p.visible = false;
   const V3<F> mc = world_to_cam(cam, mean);
@@ -530,13 +563,13 @@ GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, 
   const M3<F> cov_cam = mul(mul(cam.rot, cov3d), transpose(cam.rot));
   const M32<F> j = calc_cam_j(mc, cam);
   M2<F> cov2d = mul(mul(j, cov_cam), transpose(j));
-  opacity = opacity * compensate_cov2d(cov2d, cov_blur);
+  opacity = opacity * (hp ? compensate_cov2d_hp(cov2d, cov_blur) : compensate_cov2d(cov2d, cov_blur));
   if (opacity < F(1.0 / 255.0)) return p;
   const F rz = F(1) / mc.z;
   V2<F> mean2d;
   mean2d.x = cam.focal.x * mc.x * rz + cam.pc.x;
   mean2d.y = cam.focal.y * mc.y * rz + cam.pc.y;
-  const V3<F> conic = inverse2x2_packed(cov2d);
+  const V3<F> conic = hp ? inverse2x2_packed_hp(cov2d) : inverse2x2_packed(cov2d);
   const F thr = glog(opacity * F(255));
   const V2<F> ext = bbox_extent(cov2d, thr);
   if (ext.x < F(0) || ext.y < F(0)) return p;
@@ -577,17 +610,28 @@ template <class F> GSR_HD V3<F> view_dir(const Cam<F>& cam, V3<F> mean) {
 }
 
 // ----------------------------------------------------------------------------
-// Per-pixel blend step (rasterize.wgsl:257-276). Returns alpha, or a negative
-// value when the Gaussian does not contribute to this pixel.
+// Per-pixel blend step (rasterize.wgsl:257-276).
 // ----------------------------------------------------------------------------
-template <class F> GSR_HD F blend_alpha(F px, F py, F mx, F my, F ca, F cb, F cc, F opac, F& gauss) {
-  const F dx = mx - px, dy = my - py;
-  const F sigma = F(0.5) * (ca * dx * dx + F(2) * cb * dx * dy + cc * dy * dy);
+// sigma = 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with d = mean - pixel centre.
+template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
+  return F(0.5) * (ca * dx * dx + F(2) * cb * dx * dy + cc * dy * dy);
+}
+// alpha = min(0.999, opac * exp(-sigma)); returns it when the Gaussian
+// contributes (sigma >= 0 and alpha >= 1/255), else -1. gauss = exp(-sigma).
+template <class F> GSR_HD F blend_alpha_of(F sigma, F opac, F& gauss) {
   gauss = gexp(-sigma);
   const F alpha = gmin(F(0.999), opac * gauss);
   if (sigma >= F(0) && alpha >= F(1.0 / 255.0)) return alpha;
   return F(-1);
 }
+template <class F> GSR_HD F blend_alpha(F px, F py, F mx, F my, F ca, F cb, F cc, F opac, F& gauss) {
+  return blend_alpha_of(blend_sigma(mx - px, my - py, ca, cb, cc), opac, gauss);
+}
+// A Gaussian whose sigma exceeds log(255 * opac) + kRejectMargin cannot pass
+// the alpha >= 1/255 test: its exact alpha is below (1/255) * exp(-1e-3),
+// far outside the few-ulp error of the float exp and log. Kernels use this
+// to skip the exponential without changing any decision.
+constexpr float kRejectMargin = 1e-3f;
 
 // ----------------------------------------------------------------------------
 // Backward helpers (helpers.wgsl:79-118, 200-202, 382-427).

@@ -1,0 +1,278 @@
+// k_loss.cu — 0.8 * L1 + 0.2 * (1 - SSIM) and its gradient
+// (engine/loss.rs:42-76, 112-142, 233-276, default settings).
+//
+// SSIM uses an 11-tap sigma-1.5 normalised Gaussian window applied
+// separably (horizontal, then vertical) with replicate padding, C1 = 1e-4,
+// C2 = 9e-4 and denominators clamped at 1e-8. The reference builds it from
+// ~10 burn ops and differentiates through burn autodiff; here two tiled
+// kernels do the work:
+//  pass 1: per 32x16 output tile and channel, the five blurred moments in
+//          shared memory, the SSIM map, its partial derivatives with respect
+//          to (mu_x, E[x^2], E[xy]) and per-tile partial sums of SSIM and L1;
+//  pass 2: the adjoint of the padded separable blur applied to the three
+//          partial maps, combined with the L1 sign into d loss / d pred.
+// A last kernel reduces the per-tile sums in a fixed order (double).
+#include "gsr_kernels.h"
+
+namespace gsr {
+
+namespace {
+
+constexpr int LTX = 32, LTY = 16, R = 5, WIN = 11;
+constexpr int HX = LTX + 2 * R, HY = LTY + 2 * R;
+
+struct LossArgs {
+  const ViewDesc* views;
+  const float* pred;    // RGBA per view (pix_base)
+  const float* target;  // RGB per view (pix_base)
+  float* v_pred;
+  float* maps;          // [view][3 ch][3 maps][Pcap]
+  float* partial;       // [view][3 ch][tiles][2]
+  uint64_t Pcap;
+  uint32_t tiles_cap;
+  float k[WIN];
+  float l1_w, ssim_w;
+};
+
+__device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+__global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
+  __shared__ float s_x[HY][HX], s_y[HY][HX];
+  __shared__ float s_h[5][HY][LTX];
+  __shared__ float s_red[2][8];
+  const uint32_t v = blockIdx.z, ch = blockIdx.y;
+  const ViewDesc& vd = a.views[v];
+  const int W = (int)vd.w, H = (int)vd.h;
+  const int tiles_x = (W + LTX - 1) / LTX, tiles_y = (H + LTY - 1) / LTY;
+  const int tile = blockIdx.x;
+  if (tile >= tiles_x * tiles_y) return;
+  const int x0 = (tile % tiles_x) * LTX, y0 = (tile / tiles_x) * LTY;
+  const float* pred = a.pred + vd.pix_base * 4;
+  const float* tgt = a.target + vd.pix_base * 3;
+  for (int i = threadIdx.x; i < HX * HY; i += blockDim.x) {
+    const int hy = i / HX, hx = i % HX;
+    const int gx = clampi(x0 + hx - R, 0, W - 1), gy = clampi(y0 + hy - R, 0, H - 1);
+    const size_t p = (size_t)gy * W + gx;
+    s_x[hy][hx] = pred[p * 4 + ch];
+    s_y[hy][hx] = tgt[p * 3 + ch];
+  }
+  __syncthreads();
+  // Horizontal pass for all halo rows.
+  for (int i = threadIdx.x; i < HY * LTX; i += blockDim.x) {
+    const int hy = i / LTX, ox = i % LTX;
+    float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f, m4 = 0.f;
+#pragma unroll
+    for (int t = 0; t < WIN; ++t) {
+      const float xv = s_x[hy][ox + t], yv = s_y[hy][ox + t], w = a.k[t];
+      m0 = m0 + w * xv;
+      m1 = m1 + w * yv;
+      m2 = m2 + w * (xv * xv);
+      m3 = m3 + w * (yv * yv);
+      m4 = m4 + w * (xv * yv);
+    }
+    s_h[0][hy][ox] = m0;
+    s_h[1][hy][ox] = m1;
+    s_h[2][hy][ox] = m2;
+    s_h[3][hy][ox] = m3;
+    s_h[4][hy][ox] = m4;
+  }
+  __syncthreads();
+  const float C1 = 1e-4f, C2 = 9e-4f;
+  float ssum = 0.f, lsum = 0.f;
+  float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
+  for (int i = threadIdx.x; i < LTX * LTY; i += blockDim.x) {
+    const int oy = i / LTX, ox = i % LTX;
+    const int gx = x0 + ox, gy = y0 + oy;
+    if (gx >= W || gy >= H) continue;
+    float mx = 0.f, my = 0.f, exx = 0.f, eyy = 0.f, exy = 0.f;
+#pragma unroll
+    for (int t = 0; t < WIN; ++t) {
+      const float w = a.k[t];
+      mx = mx + w * s_h[0][oy + t][ox];
+      my = my + w * s_h[1][oy + t][ox];
+      exx = exx + w * s_h[2][oy + t][ox];
+      eyy = eyy + w * s_h[3][oy + t][ox];
+      exy = exy + w * s_h[4][oy + t][ox];
+    }
+    const float sxx = exx - mx * mx, syy = eyy - my * my, sxy = exy - mx * my;
+    const float A = 2.f * mx * my + C1, B = 2.f * sxy + C2;
+    const float Cr = mx * mx + my * my + C1, Dr = sxx + syy + C2;
+    const float Cc = fmaxf(Cr, 1e-8f), Dc = fmaxf(Dr, 1e-8f);
+    const float s = (A * B) / (Cc * Dc);
+    const float inv = 1.f / (Cc * Dc);
+    const float dC = Cr > 1e-8f ? 1.f : 0.f, dD = Dr > 1e-8f ? 1.f : 0.f;
+    const float gmx = (2.f * my * B + A * (-2.f * my)) * inv - s * ((2.f * mx * dC) * Dc + Cc * (-2.f * mx * dD)) / (Cc * Dc);
+    const float gexx = -s * dD / Dc;
+    const float gexy = 2.f * A * inv;
+    const size_t p = (size_t)gy * W + gx;
+    maps[p] = gmx;
+    maps[a.Pcap + p] = gexx;
+    maps[2 * a.Pcap + p] = gexy;
+    ssum += s;
+    lsum += fabsf(s_x[oy + R][ox + R] - s_y[oy + R][ox + R]);
+  }
+  // Fixed-order block reduction.
+  for (int o = 16; o > 0; o >>= 1) {
+    ssum += __shfl_xor_sync(0xffffffffu, ssum, o);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    s_red[0][threadIdx.x >> 5] = ssum;
+    s_red[1][threadIdx.x >> 5] = lsum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a0 = 0.f, a1 = 0.f;
+    for (int w = 0; w < 8; ++w) {
+      a0 += s_red[0][w];
+      a1 += s_red[1][w];
+    }
+    float* pp = a.partial + (((size_t)v * 3 + ch) * a.tiles_cap + tile) * 2;
+    pp[0] = a0;
+    pp[1] = a1;
+  }
+}
+
+// Weight of output q in the adjoint of a replicate-padded 11-tap
+// correlation at input p along an axis of length n.
+__device__ __forceinline__ float adj_weight(const float* k, int p, int q, int n) {
+  if (p > 0 && p < n - 1) {
+    const int d = q - p;
+    return (d >= -R && d <= R) ? k[R + d] : 0.f;
+  }
+  float w = 0.f;
+#pragma unroll
+  for (int t = 0; t < WIN; ++t)
+    if (clampi(q + t - R, 0, n - 1) == p) w += k[t];
+  return w;
+}
+
+__global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
+  __shared__ float s_g[3][HY][HX];
+  __shared__ float s_v[3][LTY][HX];
+  const uint32_t v = blockIdx.z, ch = blockIdx.y;
+  const ViewDesc& vd = a.views[v];
+  const int W = (int)vd.w, H = (int)vd.h;
+  const int tiles_x = (W + LTX - 1) / LTX, tiles_y = (H + LTY - 1) / LTY;
+  const int tile = blockIdx.x;
+  if (tile >= tiles_x * tiles_y) return;
+  const int x0 = (tile % tiles_x) * LTX, y0 = (tile / tiles_x) * LTY;
+  const float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
+  for (int i = threadIdx.x; i < HX * HY; i += blockDim.x) {
+    const int hy = i / HX, hx = i % HX;
+    const int gx = x0 + hx - R, gy = y0 + hy - R;
+    const bool ok = gx >= 0 && gx < W && gy >= 0 && gy < H;
+    const size_t p = (size_t)gy * W + gx;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) s_g[m][hy][hx] = ok ? maps[m * a.Pcap + p] : 0.f;
+  }
+  __syncthreads();
+  // Adjoint of the vertical pass: rows of the tile, all halo columns.
+  for (int i = threadIdx.x; i < LTY * HX; i += blockDim.x) {
+    const int oy = i / HX, hx = i % HX;
+    const int py = y0 + oy;
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (py < H) {
+      for (int d = -R; d <= R; ++d) {
+        const int qy = py + d;
+        if (qy < 0 || qy >= H) continue;
+        const float w = adj_weight(a.k, py, qy, H);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) acc[m] = acc[m] + w * s_g[m][oy + R + d][hx];
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) s_v[m][oy][hx] = acc[m];
+  }
+  __syncthreads();
+  const float* pred = a.pred + vd.pix_base * 4;
+  const float* tgt = a.target + vd.pix_base * 3;
+  float* out = a.v_pred + vd.pix_base * 4;
+  const float M = 3.f * (float)W * (float)H;
+  const float kl = a.l1_w / M, ks = -a.ssim_w / M;
+  for (int i = threadIdx.x; i < LTX * LTY; i += blockDim.x) {
+    const int oy = i / LTX, ox = i % LTX;
+    const int px = x0 + ox, py = y0 + oy;
+    if (px >= W || py >= H) continue;
+    float acc[3] = {0.f, 0.f, 0.f};
+    for (int d = -R; d <= R; ++d) {
+      const int qx = px + d;
+      if (qx < 0 || qx >= W) continue;
+      const float w = adj_weight(a.k, px, qx, W);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) acc[m] = acc[m] + w * s_v[m][oy][ox + R + d];
+    }
+    const size_t p = (size_t)py * W + px;
+    const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
+    const float dlt = x - y;
+    const float sg = dlt > 0.f ? 1.f : (dlt < 0.f ? -1.f : 0.f);
+    out[p * 4 + ch] = kl * sg + ks * (acc[0] + 2.f * x * acc[1] + y * acc[2]);
+    if (ch == 0) out[p * 4 + 3] = 0.f;
+  }
+}
+
+__global__ void loss_reduce_kernel(LossArgs a, uint32_t n_views, float* loss) {
+  const uint32_t v = blockIdx.x;
+  if (threadIdx.x != 0 || v >= n_views) return;
+  const ViewDesc& vd = a.views[v];
+  const int W = (int)vd.w, H = (int)vd.h;
+  const int tiles = ((W + LTX - 1) / LTX) * ((H + LTY - 1) / LTY);
+  double ss = 0.0, l1 = 0.0;
+  for (int ch = 0; ch < 3; ++ch)
+    for (int t = 0; t < tiles; ++t) {
+      const float* pp = a.partial + (((size_t)v * 3 + ch) * a.tiles_cap + t) * 2;
+      ss += pp[0];
+      l1 += pp[1];
+    }
+  const double M = 3.0 * (double)W * (double)H;
+  loss[v] = (float)((double)a.l1_w * (l1 / M) + (double)a.ssim_w * (1.0 - ss / M));
+}
+
+}  // namespace
+
+void ssim_window(float* k) {
+  // loss.rs:233-250: values in f64, stored as f32, normalised in f32.
+  float vals[WIN], sum = 0.0f;
+  for (int o = -R; o <= R; ++o) {
+    vals[o + R] = (float)exp(-(double)(o * o) / (2.0 * 1.5 * 1.5));
+    sum += vals[o + R];
+  }
+  for (int i = 0; i < WIN; ++i) k[i] = vals[i] / (sum > 1e-8f ? sum : 1e-8f);
+}
+
+uint32_t loss_tiles(uint32_t w, uint32_t h) { return ((w + LTX - 1) / LTX) * ((h + LTY - 1) / LTY); }
+
+cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const float* pred, const float* target,
+                        float l1_w, float ssim_w, float* loss, float* v_pred, float* work, uint64_t work_floats,
+                        cudaStream_t st) {
+  LossArgs a{};
+  a.views = vs.views;
+  a.pred = pred;
+  a.target = target;
+  a.v_pred = v_pred;
+  uint64_t pmax = 0;
+  uint32_t tmax = 0;
+  for (uint32_t v = 0; v < vs.n_views; ++v) {
+    const uint64_t p = (uint64_t)host_views[v].w * host_views[v].h;
+    if (p > pmax) pmax = p;
+    const uint32_t t = loss_tiles(host_views[v].w, host_views[v].h);
+    if (t > tmax) tmax = t;
+  }
+  a.Pcap = pmax;
+  a.tiles_cap = tmax;
+  const uint64_t need = (uint64_t)vs.n_views * 9 * pmax + (uint64_t)vs.n_views * 3 * tmax * 2;
+  if (need > work_floats) return cudaErrorInvalidValue;
+  a.maps = work;
+  a.partial = work + (uint64_t)vs.n_views * 9 * pmax;
+  ssim_window(a.k);
+  a.l1_w = l1_w;
+  a.ssim_w = ssim_w;
+  if (tmax == 0) return cudaSuccess;
+  dim3 grid(tmax, 3, vs.n_views);
+  ssim_fwd_kernel<<<grid, 256, 0, st>>>(a);
+  ssim_bwd_kernel<<<grid, 256, 0, st>>>(a);
+  loss_reduce_kernel<<<vs.n_views, 32, 0, st>>>(a, vs.n_views, loss);
+  return cudaGetLastError();
+}
+
+}  // namespace gsr

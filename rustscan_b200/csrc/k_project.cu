@@ -1,0 +1,154 @@
+// k_project.cu — projection, SH colour, tile counting and compaction.
+//
+// One thread per Gaussian evaluates every view of the launch: the
+// parameters are read once (the block stages its 256 x 40-byte transform
+// rows in shared memory with 128-bit loads), then for each view the thread
+// projects the Gaussian (project_forward.wgsl:19-96, project_visible.wgsl:
+// 233-310), counts the tiles it touches and the block compacts the visible
+// ones in global-id order with a decoupled look-back. This replaces the
+// atomic compaction of project_forward.wgsl:94-96 (nondeterministic order)
+// and fuses the separate project_visible pass.
+//
+// Projected record, three float4 per visible Gaussian:
+//   r0 = (x, y, conic_a, conic_b)
+//   r1 = (conic_c, opacity, red, green)
+//   r2 = (blue, log(255*opacity), tile box x0 | x1 << 16, tile box y0 | y1 << 16)
+#include <cuda_bf16.h>
+
+#include "gsr_kernels.h"
+
+namespace gsr {
+
+namespace {
+
+constexpr int kProjThreads = 256;
+
+struct ProjectArgs {
+  SplatsDev sp;
+  ViewSet vs;
+  float cov_blur;
+  int hp;
+  FwdBufs b;
+  unsigned long long* states;  // [views][parts]
+  uint32_t parts;
+  LookbackCtl* ctl;
+  DevStatus* status;
+};
+
+template <class SHT, int DEG>
+__global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
+  __shared__ float4 s_tr4[kProjThreads * 10 / 4];
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_part, s_excl;
+  const uint32_t epoch = epoch_begin(a.ctl);
+  const uint32_t part = next_ticket(a.ctl, 0, &s_part);
+  const uint32_t n = a.sp.n;
+  const uint32_t g0 = part * kProjThreads;
+  const uint32_t g = g0 + threadIdx.x;
+  const bool valid = g < n;
+  float* s_tr = reinterpret_cast<float*>(s_tr4);
+  // Stage this block's transform rows: 256 * 10 floats, 16-byte aligned.
+  {
+    const uint32_t rows = min(n - g0, (uint32_t)kProjThreads);
+    const float* src = a.sp.transforms + (size_t)g0 * 10;
+    if (rows == kProjThreads) {
+      const float4* src4 = reinterpret_cast<const float4*>(src);
+      for (int i = threadIdx.x; i < kProjThreads * 10 / 4; i += kProjThreads) s_tr4[i] = __ldg(src4 + i);
+    } else {
+      for (uint32_t i = threadIdx.x; i < rows * 10; i += kProjThreads) s_tr[i] = __ldg(src + i);
+    }
+  }
+  __syncthreads();
+  V3<float> mean{0.f, 0.f, 0.f};
+  V4<float> quat{1.f, 0.f, 0.f, 0.f};
+  V3<float> ls{0.f, 0.f, 0.f};
+  float raw = 0.f;
+  if (valid) {
+    const float* t = s_tr + threadIdx.x * 10;
+    mean = V3<float>{t[0], t[1], t[2]};
+    quat = V4<float>{t[3], t[4], t[5], t[6]};
+    ls = V3<float>{t[7], t[8], t[9]};
+    raw = __ldg(a.sp.raw_opac + g);
+  }
+  const SHT* sh = reinterpret_cast<const SHT*>(a.sp.sh);
+  constexpr int K = (DEG + 1) * (DEG + 1);
+  const TileShape ts{a.vs.tile_w, a.vs.tile_h};
+  for (uint32_t v = 0; v < a.vs.n_views; ++v) {
+    const ViewDesc& vd = a.vs.views[v];
+    const Cam<float> cam = cam_from_desc<float>(vd);
+    Projected<float> p;
+    p.visible = false;
+    uint32_t cnt = 0;
+    if (valid) {
+      p = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
+      if (p.visible) cnt = count_tiles(p, ts);
+    }
+    uint32_t tot;
+    const uint32_t rank = block_exclusive_scan(p.visible ? 1u : 0u, s_scan, &tot);
+    if (threadIdx.x == 0) {
+      s_excl = lookback(a.states + (size_t)v * a.parts, 1, part, tot, epoch, a.status, kWaitCompact);
+      if (part == a.parts - 1) a.b.vcount[v * 4 + 0] = s_excl + tot;
+    }
+    __syncthreads();
+    const uint32_t c = s_excl + rank;
+    if (valid) slice(a.b.c_of_gid, a.b.Ncap, v)[g] = p.visible ? (int32_t)c : -1;
+    if (p.visible) {
+      const SHT* shg = sh + (size_t)g * K * 3;
+      auto coeff = [&](int k, int ch) { return load_sh(shg, k * 3 + ch); };
+      const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, mean), coeff);
+      float4* r = slice(a.b.rec, a.b.Vcap * 3, v) + (size_t)c * 3;
+      r[0] = make_float4(p.mean2d.x, p.mean2d.y, p.conic.x, p.conic.y);
+      r[1] = make_float4(p.conic.z, p.opacity, rgb.x, rgb.y);
+      r[2] = make_float4(rgb.z, p.thr, __uint_as_float(p.box.x0 | (p.box.x1 << 16)),
+                         __uint_as_float(p.box.y0 | (p.box.y1 << 16)));
+      slice(a.b.gid_of_c, a.b.Vcap, v)[c] = g;
+      slice(a.b.depth_key, a.b.Vcap, v)[c] = __float_as_uint(p.depth);
+      slice(a.b.count, a.b.Vcap, v)[c] = cnt;
+    }
+  }
+  epoch_end(a.ctl, epoch);
+}
+
+template <class SHT>
+void dispatch(int degree, dim3 grid, cudaStream_t st, const ProjectArgs& a) {
+  switch (degree) {
+    case 0: project_kernel<SHT, 0><<<grid, kProjThreads, 0, st>>>(a); break;
+    case 1: project_kernel<SHT, 1><<<grid, kProjThreads, 0, st>>>(a); break;
+    case 2: project_kernel<SHT, 2><<<grid, kProjThreads, 0, st>>>(a); break;
+    case 3: project_kernel<SHT, 3><<<grid, kProjThreads, 0, st>>>(a); break;
+    default: project_kernel<SHT, 4><<<grid, kProjThreads, 0, st>>>(a); break;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blur, int fp64_conic, FwdBufs& b,
+                           const Scratch& s, cudaStream_t st) {
+  if (sp.n == 0) {
+    // No Gaussians: every view has zero visible.
+    for (uint32_t v = 0; v < vs.n_views; ++v) {
+      cudaError_t e = cudaMemsetAsync(b.vcount + v * 4, 0, 4 * sizeof(uint32_t), st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  ProjectArgs a;
+  a.sp = sp;
+  a.vs = vs;
+  a.cov_blur = cov_blur;
+  a.hp = fp64_conic;
+  a.b = b;
+  a.parts = (sp.n + kProjThreads - 1) / kProjThreads;
+  a.states = s.lb_states;
+  a.ctl = s.ctl;
+  a.status = s.status;
+  if ((uint64_t)a.parts * vs.n_views > s.lb_states_words) return cudaErrorInvalidValue;
+  dim3 grid(a.parts);
+  if (sp.sh_bf16)
+    dispatch<__nv_bfloat16>(sp.degree, grid, st, a);
+  else
+    dispatch<float>(sp.degree, grid, st, a);
+  return cudaGetLastError();
+}
+
+}  // namespace gsr

@@ -1,0 +1,360 @@
+// k_sort.cu — segmented LSD radix sort of (u32 key, u32 value) pairs and
+// decoupled-look-back scans.
+//
+// The reference sorts with a bitonic network (radix_sort.wgsl, 2 +
+// log2(P)(log2(P)+1)/2 launches of P = next_pow2(n) threads) and scans with
+// Hillis-Steele steps (prefix_sum.wgsl, 1 + log2(n) launches). Here:
+//  - one histogram pass over the keys computes the digit counts of every
+//    radix pass at once;
+//  - each radix pass is one persistent launch: blocks take 4096-key
+//    partitions by ticket, rank keys stably inside the block (warp
+//    match_any per digit, warps in order), publish per-digit counts and look
+//    back across partitions for their global offsets, then scatter through
+//    shared memory so that every digit's run is written contiguously;
+//  - scans are single-pass with the same look-back.
+// Keys are u32; `bits` limits the passes (8 bits each). Stability (ties in
+// input order) is what the reference's index tie-break provides
+// (radix_sort.wgsl:21-26).
+#include "gsr_kernels.h"
+
+namespace gsr {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kWarpKeys = kSortItems * 32;  // 512 keys per warp
+
+__device__ __forceinline__ uint32_t seg_count(const uint32_t* counts, uint32_t stride, uint32_t seg, uint32_t n_host,
+                                              uint64_t cap) {
+  if (!counts) return n_host;
+  const uint64_t c = counts[(size_t)seg * stride];
+  return (uint32_t)(c < cap ? c : cap);
+}
+
+__global__ void __launch_bounds__(256) sort_hist_kernel(const uint32_t* keys, uint64_t seg_stride,
+                                                        const uint32_t* counts, uint32_t count_stride,
+                                                        uint32_t n_host, uint64_t cap, int passes, uint32_t* hist) {
+  __shared__ uint32_t h[4][256];
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t seg = blockIdx.y;
+  const uint32_t n = seg_count(counts, count_stride, seg, n_host, cap);
+  const uint32_t* k = keys + (size_t)seg * seg_stride;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t key = k[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(key >> (8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+    const uint32_t c = (&h[0][0])[i];
+    if (c) atomicAdd(hist + (size_t)seg * 1024 + i, c);
+  }
+}
+
+__global__ void __launch_bounds__(256) sort_hist_scan_kernel(const uint32_t* hist, uint32_t* base) {
+  __shared__ uint32_t s_scan[32];
+  const uint32_t p = blockIdx.x, seg = blockIdx.y;
+  const size_t o = (size_t)seg * 1024 + p * 256 + threadIdx.x;
+  uint32_t tot;
+  base[o] = block_exclusive_scan(hist[o], s_scan, &tot);
+}
+
+struct SortPassArgs {
+  const uint32_t* keys_in;
+  const uint32_t* vals_in;  // null: values are the input positions
+  uint32_t* keys_out;
+  uint32_t* vals_out;
+  uint64_t seg_stride;
+  const uint32_t* counts;
+  uint32_t count_stride;
+  uint32_t n_host;
+  uint64_t cap;
+  uint32_t shift;
+  uint32_t pass;
+  const uint32_t* base;  // [seg][4][256]
+  unsigned long long* states;
+  uint32_t parts_cap;
+  LookbackCtl* ctl;
+  DevStatus* status;
+};
+
+__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a) {
+  __shared__ uint32_t s_keys[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];
+  __shared__ uint32_t s_whist[kSortWarps][256];
+  __shared__ uint32_t s_dstart[256];
+  __shared__ uint32_t s_gbase[256];
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_ticket;
+  const uint32_t epoch = epoch_begin(a.ctl);
+  const uint32_t seg = blockIdx.y;
+  const uint32_t n = seg_count(a.counts, a.count_stride, seg, a.n_host, a.cap);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t* kin = a.keys_in + (size_t)seg * a.seg_stride;
+  const uint32_t* vin = a.vals_in ? a.vals_in + (size_t)seg * a.seg_stride : nullptr;
+  uint32_t* kout = a.keys_out + (size_t)seg * a.seg_stride;
+  uint32_t* vout = a.vals_out + (size_t)seg * a.seg_stride;
+  unsigned long long* states = a.states + (size_t)seg * a.parts_cap * 256;
+  const uint32_t* gbase = a.base + (size_t)seg * 1024 + a.pass * 256;
+  for (;;) {
+    const uint32_t part = next_ticket(a.ctl, seg, &s_ticket);
+    if ((uint64_t)part * kSortTile >= n) break;
+    const uint32_t tile0 = part * kSortTile;
+    uint32_t key[kSortItems], val[kSortItems], lrank[kSortItems];
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i) {
+      const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
+      const bool ok = idx < n;
+      key[i] = ok ? kin[idx] : 0xffffffffu;
+      val[i] = ok ? (vin ? vin[idx] : idx) : 0u;
+    }
+    for (int j = lane; j < 256; j += 32) s_whist[warp][j] = 0;
+    __syncwarp();
+    // Stable rank within the warp: rounds in order, lanes in order.
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i) {
+      const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
+      const bool ok = idx < n;
+      const uint32_t d = ok ? ((key[i] >> a.shift) & 255u) : (256u + lane);
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t below = peers & lt_mask;
+      uint32_t b = 0;
+      if (ok) b = s_whist[warp][d];
+      __syncwarp();
+      if (ok && below == 0) s_whist[warp][d] = b + __popc(peers);
+      __syncwarp();
+      lrank[i] = b + __popc(below);
+    }
+    __syncthreads();
+    // Per digit (one per thread): warp offsets and the block count.
+    const uint32_t d = threadIdx.x;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t t = s_whist[w][d];
+      s_whist[w][d] = sum;
+      sum += t;
+    }
+    uint32_t tot;
+    const uint32_t dstart = block_exclusive_scan(sum, s_scan, &tot);
+    const uint32_t excl = lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort);
+    s_dstart[d] = dstart;
+    s_gbase[d] = gbase[d] + excl - dstart;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i) {
+      const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
+      if (idx < n) {
+        const uint32_t dd = (key[i] >> a.shift) & 255u;
+        const uint32_t pos = s_dstart[dd] + s_whist[warp][dd] + lrank[i];
+        s_keys[pos] = key[i];
+        s_vals[pos] = val[i];
+      }
+    }
+    __syncthreads();
+    const uint32_t nvalid = min((uint32_t)kSortTile, n - tile0);
+    for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
+      const uint32_t k = s_keys[j];
+      const uint32_t dst = s_gbase[(k >> a.shift) & 255u] + j;
+      kout[dst] = k;
+      vout[dst] = s_vals[j];
+    }
+  }
+  epoch_end(a.ctl, epoch);
+}
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back scan: 2048 elements per partition, thread-striped
+// rounds. in[gather[i]] when gather is set. Exclusive or inclusive output.
+// Per segment totals: totals[seg * tstride + 0] = min(total, cap_total),
+// totals[seg * tstride + 1] = total; overflow is flagged when total exceeds
+// cap_total.
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+struct ScanArgs {
+  const uint32_t* in;
+  const uint32_t* gather;
+  uint32_t* out;
+  uint64_t seg_stride;
+  const uint32_t* counts;
+  uint32_t count_stride;
+  uint32_t n_host;
+  uint64_t cap;
+  int inclusive;
+  uint32_t* totals;
+  uint32_t totals_stride;
+  uint64_t cap_total;
+  unsigned long long* states;
+  uint32_t parts_cap;
+  LookbackCtl* ctl;
+  DevStatus* status;
+};
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_ticket, s_excl;
+  const uint32_t epoch = epoch_begin(a.ctl);
+  const uint32_t seg = blockIdx.y;
+  const uint32_t n = seg_count(a.counts, a.count_stride, seg, a.n_host, a.cap);
+  const uint32_t* in = a.in + (size_t)seg * a.seg_stride;
+  const uint32_t* ga = a.gather ? a.gather + (size_t)seg * a.seg_stride : nullptr;
+  uint32_t* out = a.out + (size_t)seg * a.seg_stride;
+  unsigned long long* states = a.states + (size_t)seg * a.parts_cap;
+  const uint32_t nparts = (n + kScanTile - 1) / kScanTile;
+  if (n == 0 && a.totals && blockIdx.x == 0 && threadIdx.x == 0) {
+    a.totals[(size_t)seg * a.totals_stride + 0] = 0;
+    a.totals[(size_t)seg * a.totals_stride + 1] = 0;
+  }
+  for (;;) {
+    const uint32_t part = next_ticket(a.ctl, seg, &s_ticket);
+    if (part >= nparts) break;
+    const uint32_t tile0 = part * kScanTile;
+    uint32_t v[kScanItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const uint32_t idx = tile0 + i * kScanThreads + threadIdx.x;
+      v[i] = (idx < n) ? (ga ? in[ga[idx]] : in[idx]) : 0u;
+    }
+    // Rounds in order; within a round threads in order.
+    uint32_t round_base[kScanItems];
+    uint32_t carry = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      uint32_t tot;
+      const uint32_t e = block_exclusive_scan(v[i], s_scan, &tot);
+      round_base[i] = carry + e;
+      carry += tot;
+    }
+    local = carry;
+    if (threadIdx.x == 0) s_excl = lookback(states, 1, part, local, epoch, a.status, kWaitScan);
+    __syncthreads();
+    const uint32_t excl = s_excl;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const uint32_t idx = tile0 + i * kScanThreads + threadIdx.x;
+      if (idx < n) out[idx] = excl + round_base[i] + (a.inclusive ? v[i] : 0u);
+    }
+    if (part == nparts - 1 && threadIdx.x == 0 && a.totals) {
+      const uint64_t total = (uint64_t)excl + local;
+      a.totals[(size_t)seg * a.totals_stride + 0] = (uint32_t)(total < a.cap_total ? total : a.cap_total);
+      a.totals[(size_t)seg * a.totals_stride + 1] = (uint32_t)total;
+      if (total > a.cap_total) {
+        atomicExch(&a.status->overflow, 1u);
+        atomicMax(&a.status->required, (unsigned long long)total);
+      }
+    }
+  }
+  epoch_end(a.ctl, epoch);
+}
+
+int persistent_blocks(int num_sms, uint32_t segments, int per_sm) {
+  const int total = num_sms * per_sm;
+  const int per = total / (int)(segments ? segments : 1);
+  return per < 1 ? 1 : per;
+}
+
+}  // namespace
+
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                             uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride, uint32_t segments,
+                             const uint32_t* counts, uint32_t count_stride, uint32_t n_host, uint64_t cap_per_segment,
+                             int bits, const Scratch& s, cudaStream_t st) {
+  if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
+  int passes = (bits + 7) / 8;
+  if (passes < 1) passes = 1;
+  if (passes > 4) passes = 4;
+  const uint32_t parts_cap = (uint32_t)((cap_per_segment + kSortTile - 1) / kSortTile);
+  if ((uint64_t)parts_cap * 256 * segments > s.lb_states_words) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 1024 * segments, st);
+  if (e != cudaSuccess) return e;
+  {
+    dim3 grid(persistent_blocks(s.num_sms, segments, 4), segments);
+    sort_hist_kernel<<<grid, 256, 0, st>>>(keys_in, seg_stride, counts, count_stride, n_host, cap_per_segment, passes,
+                                           s.hist);
+  }
+  sort_hist_scan_kernel<<<dim3(passes, segments), 256, 0, st>>>(s.hist, s.hist_base);
+  // Ping-pong so that the last pass writes keys_out/vals_out.
+  const uint32_t* ki = keys_in;
+  const uint32_t* vi = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint32_t* ko = to_out ? keys_out : keys_tmp;
+    uint32_t* vo = to_out ? vals_out : vals_tmp;
+    SortPassArgs a;
+    a.keys_in = ki;
+    a.vals_in = vi;
+    a.keys_out = ko;
+    a.vals_out = vo;
+    a.seg_stride = seg_stride;
+    a.counts = counts;
+    a.count_stride = count_stride;
+    a.n_host = n_host;
+    a.cap = cap_per_segment;
+    a.shift = 8 * p;
+    a.pass = p;
+    a.base = s.hist_base;
+    a.states = s.lb_states;
+    a.parts_cap = parts_cap;
+    a.ctl = s.ctl;
+    a.status = s.status;
+    dim3 grid(persistent_blocks(s.num_sms, segments, 3), segments);
+    sort_pass_kernel<<<grid, kSortThreads, 0, st>>>(a);
+    ki = ko;
+    vi = vo;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_host, const Scratch& s,
+                               cudaStream_t st) {
+  if (n_host == 0) return cudaSuccess;
+  ScanArgs a{};
+  a.in = in;
+  a.gather = nullptr;
+  a.out = out;
+  a.seg_stride = 0;
+  a.counts = nullptr;
+  a.n_host = n_host;
+  a.cap = n_host;
+  a.inclusive = 1;
+  a.totals = nullptr;
+  a.parts_cap = (n_host + kScanTile - 1) / kScanTile;
+  if (a.parts_cap > s.lb_states_words) return cudaErrorInvalidValue;
+  a.states = s.lb_states;
+  a.ctl = s.ctl;
+  a.status = s.status;
+  scan_kernel<<<dim3(persistent_blocks(s.num_sms, 1, 4), 1), kScanThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
+  ScanArgs a{};
+  a.in = b.count;
+  a.gather = b.perm;
+  a.out = b.offset;
+  a.seg_stride = b.Vcap;
+  a.counts = b.vcount;
+  a.count_stride = 4;
+  a.cap = b.Vcap;
+  a.inclusive = 0;
+  a.totals = b.vcount + 1;
+  a.totals_stride = 4;
+  a.cap_total = b.Icap;
+  a.parts_cap = (uint32_t)((b.Vcap + kScanTile - 1) / kScanTile);
+  if ((uint64_t)a.parts_cap * vs.n_views > s.lb_states_words) return cudaErrorInvalidValue;
+  a.states = s.lb_states;
+  a.ctl = s.ctl;
+  a.status = s.status;
+  scan_kernel<<<dim3(persistent_blocks(s.num_sms, vs.n_views, 4), vs.n_views), kScanThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace gsr

@@ -1,0 +1,237 @@
+"""CPU checks of the oracle itself: the reference's own known answers, an
+independent numpy restatement of the projection, the portable exp/log, FP64
+finite differences of the exact adjoint, and agreement of the reverse-walk
+reference mode with the literal WGSL backward walk."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rustscan_b200 import scenes as S
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_known_answers.json")))
+
+
+@pytest.mark.parametrize("case", GOLD["prefix_sum"], ids=lambda c: c["test"])
+def test_prefix_sum_known_answers(case):
+    np.testing.assert_array_equal(O.prefix_sum_u32(case["input"]), np.asarray(case["expected"], np.uint32))
+
+
+@pytest.mark.parametrize("case", GOLD["argsort"], ids=lambda c: c["test"])
+def test_argsort_known_answers(case):
+    _, v = O.sort_pairs_u32(case["keys"], np.arange(len(case["keys"])))
+    np.testing.assert_array_equal(v, np.asarray(case["expected"], np.uint32))
+
+
+def test_sort_by_key_known_answer():
+    c = GOLD["sort_by_key"][0]
+    k, v = O.sort_pairs_u32(c["keys"], c["values"])
+    np.testing.assert_array_equal(k, c["expected_keys"])
+    np.testing.assert_array_equal(v, c["expected_values"])
+
+
+def test_sh_degree0_identity():
+    """sh/tests.rs:3-9: degree-0 SH of rgb_to_sh0(rgb) is rgb (through a splat's colour)."""
+    rgb = np.asarray(GOLD["sh_degree0_identity"]["rgb"], np.float32)
+    cam = S.camera_from_rt(np.eye(3), np.array([0.0, 0.0, 2.0]), 100, 100, 8, 8, 16, 16)
+    tr = np.array([[0, 0, 0, 1, 0, 0, 0, -2, -2, -2]], np.float32)
+    sh = ((rgb - 0.5) / np.float32(S.SH_C0)).astype(np.float32).reshape(1, 1, 3)
+    f = O.Forward(tr, sh, np.array([3.0], np.float32), 0, cam)
+    np.testing.assert_allclose(f.rec[0, 7:10], rgb, atol=1e-6)
+
+
+def test_camera_projects_principal_point():
+    """core/camera_tests.rs:12-25: (0,0,1) projects to the principal point."""
+    c = GOLD["camera_project"]
+    W, H, f = c["width"], c["height"], c["focal"]
+    cam = S.camera_from_rt(np.eye(3), np.zeros(3), f, f, W / 2, H / 2, W, H)
+    tr = np.array([[0, 0, 1, 1, 0, 0, 0, -3, -3, -3]], np.float32)
+    fw = O.Forward(tr, np.zeros((1, 1, 3), np.float32), np.array([2.0], np.float32), 0, cam)
+    assert fw.num_visible == 1
+    np.testing.assert_allclose(fw.rec[0, :2], c["expected_pixel"], atol=c["tolerance"])
+
+
+def test_portable_exp_log_accuracy():
+    xs = np.concatenate([np.linspace(-87.3, 88.7, 20001), np.random.default_rng(0).uniform(-30, 5, 20000)])
+    worst = 0.0
+    for x in xs.astype(np.float32):
+        e = O.expf(x)
+        ref = math.exp(float(x))
+        if ref > 1.2e-38:
+            worst = max(worst, abs(e - ref) / (np.spacing(np.float32(ref))))
+    assert worst <= 2.0, worst
+    worst = 0.0
+    for x in np.concatenate([np.geomspace(1e-30, 1e30, 20001), np.linspace(0.5, 2.0, 5001)]).astype(np.float32):
+        lg = O.logf(x)
+        ref = math.log(float(x))
+        err = abs(lg - ref) / max(float(np.spacing(np.float32(abs(ref)))), 1e-9)
+        worst = max(worst, err)
+    assert worst <= 2.0, worst
+
+
+def _numpy_project(tr, raw, cam, blur=0.3):
+    """Independent float64 restatement of project_forward.wgsl:19-73."""
+    M = cam.viewmat.astype(np.float64).reshape(4, 4).T
+    R, t = M[:3, :3], M[:3, 3]
+    mean = tr[:3].astype(np.float64)
+    mc = R @ mean + t
+    q = tr[3:7].astype(np.float64)
+    q = q / np.linalg.norm(q)
+    w, x, y, z = q
+    Rq = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                   [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                   [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+    Mm = Rq @ np.diag(np.exp(tr[7:10].astype(np.float64)))
+    cov = R @ (Mm @ Mm.T) @ R.T
+    # The camera record carries float32 intrinsics.
+    fx, fy, cx, cy = (float(np.float32(a)) for a in (cam.fx, cam.fy, cam.cx, cam.cy))
+    rz = 1 / mc[2]
+    lx = ((1.15 * cam.width - cx) / fx, (-0.15 * cam.width - cx) / fx)
+    ly = ((1.15 * cam.height - cy) / fy, (-0.15 * cam.height - cy) / fy)
+    u = min(max(mc[0] * rz, lx[1]), lx[0])
+    v = min(max(mc[1] * rz, ly[1]), ly[0])
+    J = np.array([[fx * rz, 0, -fx * rz * u], [0, fy * rz, -fy * rz * v]])
+    c2 = J @ cov @ J.T
+    d0 = np.linalg.det(c2)
+    c2b = c2 + blur * np.eye(2)
+    comp = math.sqrt(d0 / np.linalg.det(c2b))
+    op = comp / (1 + math.exp(-raw))
+    reg = c2b + 1e-6 * np.eye(2)
+    inv = np.linalg.inv(reg)
+    mean2d = (fx * mc[0] * rz + cx, fy * mc[1] * rz + cy)
+    return mean2d, (inv[0, 0], inv[0, 1], inv[1, 1]), op, mc[2]
+
+
+def test_projection_matches_independent_numpy():
+    sc = S.small_scene(n=200, degree=1, width=80, height=60, seed=2, logscale_mu=-2.5)
+    cam = sc.cameras[0]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 1, cam, f64=True)
+    assert f.num_visible > 50
+    for c, g in enumerate(f.gid):
+        m2, con, op, z = _numpy_project(sc.transforms[g], float(sc.raw_opacity[g]), cam)
+        np.testing.assert_allclose(f.rec[c, 0:2], m2, rtol=1e-10)
+        np.testing.assert_allclose(f.rec[c, 2:5], con, rtol=1e-8, atol=1e-12)
+        np.testing.assert_allclose(f.rec[c, 5], op, rtol=1e-10)
+        np.testing.assert_allclose(f.depth[c], z, rtol=1e-12)
+
+
+def test_f32_oracle_close_to_f64():
+    sc = S.config1(n=4000)
+    cam = sc.cameras[0]
+    a = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 0, cam)
+    b = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 0, cam, f64=True)
+    assert abs(a.num_visible - b.num_visible) <= 2
+    assert np.abs(a.image - b.image).max() < 1e-3
+    psnr = -10 * math.log10(float(np.mean((a.image[..., :3] - b.image[..., :3]) ** 2)) + 1e-30)
+    assert psnr > 80
+
+
+def _fd_scene():
+    sc = S.small_scene(n=200, degree=3, width=48, height=40, seed=3, logscale_mu=-2.5)
+    g = S.upstream_grad(40, 48).astype(np.float64)
+    g[..., 3] = np.random.default_rng(1).standard_normal(g[..., 3].shape) * 0.5
+    return sc, g
+
+
+def test_exact_adjoint_matches_fp64_finite_differences():
+    """Central differences (step 1e-5) on 40 random visible parameters."""
+    sc, g = _fd_scene()
+    cam = sc.cameras[0]
+    tr, sh, op = (a.astype(np.float64) for a in (sc.transforms, sc.sh, sc.raw_opacity))
+
+    def L(tr_, sh_, op_):
+        return float((O.Forward(tr_, sh_, op_, 3, cam, f64=True).image * g).sum())
+
+    f = O.Forward(tr, sh, op, 3, cam, f64=True)
+    b = f.backward(g, mode=0)
+    rng = np.random.default_rng(0)
+    errs = []
+    h = 1e-5
+    for _ in range(40):
+        gi = int(rng.choice(f.gid))
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            j = int(rng.integers(0, 10))
+            a, c = tr.copy(), tr.copy()
+            a[gi, j] += h
+            c[gi, j] -= h
+            fd, an = (L(a, sh, op) - L(c, sh, op)) / (2 * h), b["v_transforms"][gi, j]
+        elif kind == 1:
+            k, ch = int(rng.integers(0, 16)), int(rng.integers(0, 3))
+            a, c = sh.copy(), sh.copy()
+            a[gi, k, ch] += h
+            c[gi, k, ch] -= h
+            fd, an = (L(tr, a, op) - L(tr, c, op)) / (2 * h), b["v_sh"][gi, k, ch]
+        else:
+            a, c = op.copy(), op.copy()
+            a[gi] += h
+            c[gi] -= h
+            fd, an = (L(tr, sh, a) - L(tr, sh, c)) / (2 * h), b["v_raw_opacity"][gi]
+        errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-6))
+    errs = np.asarray(errs)
+    assert np.median(errs) < 1e-6 and np.quantile(errs, 0.9) < 1e-4, errs
+
+
+def test_reference_mode_equals_literal_wgsl_walk():
+    sc = S.small_scene(n=1500, degree=2, width=64, height=48, seed=8)
+    cam = sc.cameras[0]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 2, cam, f64=True)
+    g = S.upstream_grad(48, 64).astype(np.float64)
+    b1 = f.backward(g, mode=1)
+    b2 = f.backward(g, mode=2)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity", "stats"):
+        np.testing.assert_allclose(b1[k], b2[k], rtol=1e-7, atol=1e-9 * max(1.0, np.abs(b2[k]).max()))
+
+
+def test_loss_gradient_matches_finite_differences():
+    rng = np.random.default_rng(4)
+    H, W = 20, 24
+    pred = rng.uniform(0, 1, (H, W, 4))
+    tgt = rng.uniform(0, 1, (H, W, 3))
+    val, v = O.loss(pred, tgt, f64=True)
+    h = 1e-6
+    for _ in range(30):
+        y, x, c = int(rng.integers(0, H)), int(rng.integers(0, W)), int(rng.integers(0, 3))
+        a, b = pred.copy(), pred.copy()
+        a[y, x, c] += h
+        b[y, x, c] -= h
+        fd = (O.loss(a, tgt, f64=True)[0] - O.loss(b, tgt, f64=True)[0]) / (2 * h)
+        assert abs(fd - v[y, x, c]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (fd, v[y, x, c])
+    assert np.all(v[..., 3] == 0)
+
+
+def test_ssim_of_identical_images_is_zero_loss():
+    """engine/loss_tests.rs: SSIM loss of identical images is ~0."""
+    img = np.random.default_rng(3).uniform(0, 1, (32, 32, 3))
+    val, _ = O.loss(img, img, l1_weight=0.0, ssim_weight=1.0, f64=True)
+    assert abs(val) < 1e-9
+
+
+def test_adam_decreases_param_with_positive_grad():
+    """engine/optimizer_tests.rs:9-32."""
+    p = np.ones(10, np.float32)
+    O.adam(p, np.ones(10, np.float32), np.zeros(10, np.float32), np.zeros(10, np.float32), [0.1], 1)
+    assert np.all(p < 1.0)
+
+
+def test_adam_matches_numpy_restatement():
+    rng = np.random.default_rng(7)
+    p0 = rng.standard_normal(100).astype(np.float32)
+    p = p0.copy()
+    m = np.zeros(100, np.float32)
+    v = np.zeros(100, np.float32)
+    mr, vr, pr = m.copy(), v.copy(), p0.copy()
+    for step in range(1, 5):
+        g = rng.standard_normal(100).astype(np.float32)
+        O.adam(p, g, m, v, [0.01, 0.02], step)
+        b1, b2 = np.float32(0.9), np.float32(0.999)
+        mr = mr * b1 + g * (np.float32(1) - b1)
+        vr = vr * b2 + (g * g) * (np.float32(1) - b2)
+        bc1 = np.float32(1) - b1 ** np.float32(step)
+        bc2 = np.float32(1) - b2 ** np.float32(step)
+        upd = (mr / bc1) / (np.sqrt(vr / bc2) + np.float32(1e-8))
+        pr = pr - upd * np.tile(np.float32([0.01, 0.02]), 50)
+    np.testing.assert_allclose(p, pr, rtol=1e-5, atol=1e-6)
