@@ -58,6 +58,7 @@ struct gsr_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<uint8_t> graph_key;
   int graph_kernels = 0;
+  cudaStream_t capture_stream = nullptr;  // graphs are recorded here (the legacy default stream cannot capture)
   // optional stage timing (events recorded between stages; never in a graph)
   bool prof_on = false;
   std::vector<int> prof_stage;
@@ -125,6 +126,8 @@ void free_all(gsr_ctx* c) {
   c->allocs.clear();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   c->graph_exec = nullptr;
+  if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
+  c->capture_stream = nullptr;
 }
 
 uint64_t tcap_for(const gsr_config& cfg) { return cfg.max_pixels / ((uint64_t)cfg.tile_w * cfg.tile_h) + 4096; }
@@ -635,7 +638,6 @@ gsr_status gsr_train_step(gsr_ctx* c, float* transforms, void* sh, float* raw_op
   put(&p->l1_weight, 4);
   put(&p->ssim_weight, 4);
   put(&p->use_visible, 4);
-  put(&st, sizeof(st));
   if (c->graph_exec == nullptr || key != c->graph_key) {
     if (c->graph_exec) {
       cudaGraphExecDestroy(c->graph_exec);
@@ -646,9 +648,11 @@ gsr_status gsr_train_step(gsr_ctx* c, float* transforms, void* sh, float* raw_op
     gsr_status rs = build_views(c, cams, n_views, desc, vs);
     if (rs != GSR_OK) return rs;
     cudaGraph_t graph = nullptr;
-    GSR_CUDA(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    rs = train_body(c, &sp, transforms, sh, raw_opacity, state, cams, n_views, targets, p, densify_acc, loss, st);
-    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (!c->capture_stream) GSR_CUDA(c, cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = c->capture_stream;
+    GSR_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    rs = train_body(c, &sp, transforms, sh, raw_opacity, state, cams, n_views, targets, p, densify_acc, loss, cs);
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
     if (rs != GSR_OK) {
       if (graph) cudaGraphDestroy(graph);
       return rs;
