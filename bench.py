@@ -39,6 +39,8 @@ def parse():
     p.add_argument("--views", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--mode", default="bench", choices=["bench", "profile"],
+                   help="profile: warm up, then run exactly one non-graph batched step (for ncu launch lists)")
     return p.parse_args()
 
 
@@ -257,6 +259,30 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_step(args):
+    """Warm-up steps, then one batched step without a graph: every kernel of
+    the step appears once in a profiler's launch list after the warm-up."""
+    import torch
+
+    from rustscan_b200 import LearningRates, Trainer, host_splats_to_device
+    from rustscan_b200 import scenes as S
+
+    sc = S.config3(n=args.n, views=args.views)
+    cams = sc.cameras
+    H, W = cams[0].height, cams[0].width
+    ctx = make_context(args.n, len(cams))
+    splats = host_splats_to_device(sc)
+    fit_capacity(ctx, splats, cams)
+    rng = np.random.default_rng(0)
+    targets = torch.as_tensor(rng.uniform(0, 1, (len(cams), H, W, 3)).astype(np.float32), device="cuda")
+    tr = Trainer(ctx, splats, LearningRates(), use_graph=False)
+    for i in range(args.warmup + 1):
+        tr.train_step(cams, targets, i + 1)
+    torch.cuda.synchronize()
+    ctx.sync_status()
+    print(json.dumps({"profile_step": "done", "views": len(cams), "n": args.n}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -268,6 +294,9 @@ def main():
     from rustscan_b200 import scenes as S
 
     world, rank, local = dist_setup(args)
+    if args.mode == "profile":
+        profile_step(args)
+        return
     sc = S.config3(seed_offset=rank, n=args.n, views=args.views)
     gt_tr, gt_sh, gt_op = S.config3_targets(seed_offset=rank, n=args.n)
     cams = sc.cameras
