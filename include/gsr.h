@@ -123,6 +123,27 @@ GSR_API gsr_status gsr_reserve_isects(gsr_ctx* ctx, uint64_t max_isects);
  * not alias. n <= 2^30. */
 GSR_API gsr_status gsr_prefix_sum_u32(gsr_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t n, void* stream);
 
+/* Inclusive scan of n u32 values that allocates no device memory and needs no
+ * context. No counterpart in the reference: it exists for callers that must
+ * not have a library allocate on their behalf, such as host frameworks that
+ * own the whole device memory budget through their own pool (an allocation
+ * outside it breaks their accounting or fails mid-run) and deployments that
+ * fix their memory use at start-up.
+ * Limits and behaviour:
+ *  - n <= 16,777,216 (2^24); larger n returns GSR_ERR_INVALID_ARG.
+ *  - Scratch is a 64 KiB array compiled into libgsr (a file-scope __device__
+ *    variable) that every GPU loading the library keeps until process exit.
+ *  - The first call on each device looks up that array's device address
+ *    (cudaGetSymbolAddress) with the device current; make that first call
+ *    before any stream capture.
+ *  - All calls on a device share the one array: calls whose work overlaps
+ *    on the GPU (different streams, or threads) race and give wrong results.
+ *    Serialise them, e.g. on one stream.
+ *  - It only enqueues work; a device-side wait that gives up cannot be
+ *    reported here (results are then wrong but the call still finishes).
+ * in and out are device pointers and may not alias. */
+GSR_API gsr_status gsr_prefix_sum_u32_noalloc(const uint32_t* in, uint32_t* out, uint32_t n, void* stream);
+
 /* Stable ascending sort of (key, value) pairs; equal keys keep input order.
  * Replaces RadixSortBackend::radix_sort_by_key_u32_primitive
  * (RustGS/src/training/gpu_primitives/radix_sort.rs:48-53). Inputs are not

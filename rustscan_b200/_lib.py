@@ -118,6 +118,7 @@ EXPORTED = [
     "gsr_sync_status",
     "gsr_reserve_isects",
     "gsr_prefix_sum_u32",
+    "gsr_prefix_sum_u32_noalloc",
     "gsr_radix_sort_by_key_u32",
     "gsr_render_forward",
     "gsr_render_backward",
@@ -161,6 +162,7 @@ def load():
     L.gsr_sync_status.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
     L.gsr_reserve_isects.argtypes = [vp, C.c_uint64]
     L.gsr_prefix_sum_u32.argtypes = [vp, vp, vp, u32, vp]
+    L.gsr_prefix_sum_u32_noalloc.argtypes = [vp, vp, u32, vp]
     L.gsr_radix_sort_by_key_u32.argtypes = [vp, vp, vp, vp, vp, u32, vp]
     L.gsr_render_forward.argtypes = [vp, C.POINTER(gsr_splats), C.POINTER(gsr_camera), u32, vp, vp, vp]
     L.gsr_render_backward.argtypes = [vp, C.POINTER(gsr_splats), vp, C.POINTER(gsr_grads), vp, vp]

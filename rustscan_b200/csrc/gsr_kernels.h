@@ -89,6 +89,11 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
 cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_host, const Scratch& s,
                                cudaStream_t st);
 
+// The same scan with caller-provided look-back scratch (no context).
+cudaError_t inclusive_scan_u32_scratch(const uint32_t* in, uint32_t* out, uint32_t n_host, unsigned long long* states,
+                                       uint64_t states_words, LookbackCtl* ctl, DevStatus* status, int num_sms,
+                                       cudaStream_t st);
+
 // Per view: offset[r] = exclusive scan of count[perm[r]], sets vcount[1..2].
 cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 

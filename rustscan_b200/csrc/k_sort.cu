@@ -335,6 +335,29 @@ cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_hos
   return cudaGetLastError();
 }
 
+cudaError_t inclusive_scan_u32_scratch(const uint32_t* in, uint32_t* out, uint32_t n_host, unsigned long long* states,
+                                       uint64_t states_words, LookbackCtl* ctl, DevStatus* status, int num_sms,
+                                       cudaStream_t st) {
+  if (n_host == 0) return cudaSuccess;
+  ScanArgs a{};
+  a.in = in;
+  a.gather = nullptr;
+  a.out = out;
+  a.seg_stride = 0;
+  a.counts = nullptr;
+  a.n_host = n_host;
+  a.cap = n_host;
+  a.inclusive = 1;
+  a.totals = nullptr;
+  a.parts_cap = (n_host + kScanTile - 1) / kScanTile;
+  if (a.parts_cap > states_words) return cudaErrorInvalidValue;
+  a.states = states;
+  a.ctl = ctl;
+  a.status = status;
+  scan_kernel<<<dim3(persistent_blocks(num_sms, 1, 4), 1), kScanThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
   ScanArgs a{};
   a.in = b.count;
