@@ -222,9 +222,9 @@ template <class F> void forward(FwdState<F>& st) {
               blend_alpha(pcx, pcy, p.mean2d.x, p.mean2d.y, p.conic.x, p.conic.y, p.conic.z, p.opacity, gauss);
           if (alpha < F(0)) continue;
           const F vis = alpha * Tr;
-          C[0] = C[0] + gmax(st.rgb[c].x, F(0)) * vis;
-          C[1] = C[1] + gmax(st.rgb[c].y, F(0)) * vis;
-          C[2] = C[2] + gmax(st.rgb[c].z, F(0)) * vis;
+          C[0] = blend_accum(C[0], st.rgb[c].x, vis);
+          C[1] = blend_accum(C[1], st.rgb[c].y, vis);
+          C[2] = blend_accum(C[2], st.rgb[c].z, vis);
           Tr = Tr * (F(1) - alpha);
           vis_c[c] = 1;  // benign race: every writer stores 1
           last = s + 1;
@@ -701,14 +701,16 @@ ORC_FWD_IMPL(f64, double)
 ORC_EXPORT void orc_adam_f32(float* p, const float* g, float* m, float* v, uint64_t n, const float* lr, int ncols,
                              int step, float beta1, float beta2, float eps) {
   const float omb1 = 1.0f - beta1, omb2 = 1.0f - beta2;
-  const float bc1 = 1.0f - powi_f32(beta1, step), bc2 = 1.0f - powi_f32(beta2, step);
+  // The bias corrections are applied as multiplications by their f32
+  // reciprocals (the reference divides; the two differ by at most an ulp).
+  const float rbc1 = 1.0f / (1.0f - powi_f32(beta1, step)), rbc2 = 1.0f / (1.0f - powi_f32(beta2, step));
   for (uint64_t i = 0; i < n; ++i) {
     const float gi = g[i];
     const float m1 = m[i] * beta1 + gi * omb1;
     const float m2 = v[i] * beta2 + (gi * gi) * omb2;
     m[i] = m1;
     v[i] = m2;
-    const float mh = m1 / bc1, vh = m2 / bc2;
+    const float mh = m1 * rbc1, vh = m2 * rbc2;
     const float upd = mh / (sqrtf(vh) + eps);
     p[i] = p[i] - upd * lr[i % (uint64_t)ncols];
   }

@@ -53,6 +53,8 @@ struct gsr_ctx {
   float* v_render = nullptr;
   float* loss_work = nullptr;
   uint64_t loss_work_floats = 0;
+  float* grad_work = nullptr;  // summed gradient of a training step: [N][10], [N][3K<=75], [N] (16-byte aligned)
+  uint64_t grad_sh_off = 0, grad_op_off = 0;
   AdamScalars* d_scal = nullptr;
   // graph cache of the training step
   cudaGraphExec_t graph_exec = nullptr;
@@ -151,7 +153,7 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.isect_key_raw, nv * I) && dalloc(c, &b.isect_val_raw, nv * I) &&
             dalloc(c, &b.ranges, nv * 2 * T) && dalloc(c, &b.tfinal, nv * P) && dalloc(c, &b.last, nv * P) &&
             dalloc(c, &b.ncontrib, nv * P) && dalloc(c, &b.nvisit, nv * P) && dalloc(c, &b.visible_c, nv * V) &&
-            dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.vcount, nv * 4);
+            dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4);
   if (ok && cfg.deterministic)
     ok = dalloc(c, &b.sgrad_part, nv * I * 12) && dalloc(c, &b.inv_perm, nv * I);
   else {
@@ -169,8 +171,10 @@ gsr_status allocate(gsr_ctx* c) {
        dalloc(c, &c->d_views, nv) && dalloc(c, &c->d_scal, 1);
   const uint64_t lt = loss_tiles(1, 1) + P / (32 * 16) + 2 * (P / 16) + 64;
   c->loss_work_floats = nv * 9 * P + nv * 3 * lt * 2;
+  c->grad_sh_off = (N * 10 + 3) & ~uint64_t(3);
+  c->grad_op_off = c->grad_sh_off + ((N * 75 + 3) & ~uint64_t(3));
   ok = ok && dalloc(c, &c->render, nv * P * 4) && dalloc(c, &c->v_render, nv * P * 4) &&
-       dalloc(c, &c->loss_work, c->loss_work_floats);
+       dalloc(c, &c->loss_work, c->loss_work_floats) && dalloc(c, &c->grad_work, c->grad_op_off + N);
   if (!ok) return fail(c, GSR_ERR_OOM, "device allocation failed (reduce max_splats/max_isects/max_pixels)");
   c->s.lb_states_words = c->states_words;
   c->s.num_sms = c->num_sms;
@@ -464,7 +468,7 @@ gsr_status gsr_render_backward(gsr_ctx* c, const gsr_splats* sp, const float* v_
   pa.grad_scale = 1.0f;
   pa.exact = c->cfg.adjoint == GSR_ADJOINT_EXACT;
   prof_mark(c, kStProjectBwd, st);
-  GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, nullptr, st, c->num_sms));
+  GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, st, c->num_sms));
   prof_mark(c, kStCount, st);
   return GSR_OK;
 }
@@ -536,9 +540,10 @@ static AdamScalars make_scalars(const gsr_lr* lr, int32_t step) {
   s.beta1 = lr->beta1;
   s.beta2 = lr->beta2;
   s.eps = lr->eps;
-  // engine/optimizer.rs:144-147: 1 - beta^step with f32 powi.
-  s.bc1 = 1.0f - powi_f32(lr->beta1, step);
-  s.bc2 = 1.0f - powi_f32(lr->beta2, step);
+  // engine/optimizer.rs:144-147: 1 - beta^step with f32 powi; the kernels
+  // multiply by the f32 reciprocals.
+  s.rbc1 = 1.0f / (1.0f - powi_f32(lr->beta1, step));
+  s.rbc2 = 1.0f / (1.0f - powi_f32(lr->beta2, step));
   return s;
 }
 
@@ -598,12 +603,18 @@ static gsr_status train_body(gsr_ctx* c, const gsr_splats* sp, float* transforms
   a.v_op = state->v_opacity;
   a.scal = c->d_scal;
   ProjBwdArgs pa{};
+  pa.v_tr = c->grad_work;
+  pa.v_sh = c->grad_work + c->grad_sh_off;
+  pa.v_op = c->grad_work + c->grad_op_off;
   pa.densify_acc = densify_acc;
   pa.use_visible = p->use_visible;
   pa.grad_scale = 1.0f / (float)n_views;
   pa.exact = c->cfg.adjoint == GSR_ADJOINT_EXACT;
+  prof_mark(c, kStProjectBwd, st);
+  GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, st, c->num_sms));
   prof_mark(c, kStAdam, st);
-  GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, &a, st, c->num_sms));
+  GSR_CUDA(c, launch_adam(a, pa.v_tr, pa.v_sh, pa.v_op, sp->n, (int)sp->sh_degree, c->cfg.sh_dtype == GSR_SH_BF16,
+                          st, c->num_sms));
   prof_mark(c, kStCount, st);
   return GSR_OK;
 }

@@ -34,6 +34,7 @@ struct FwdBufs {
   uint32_t* nvisit;        // [P]
   uint8_t* visible_c;      // [V]
   float4* sgrad;           // [V][3] screen-space gradient sums (12 floats)
+  float4* pair;            // [views][6][Vcap]: six float4 planes of projection adjoint records
   float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)
   uint32_t* inv_perm;      // [I] emission index -> sorted position (deterministic mode)
   uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
@@ -120,7 +121,8 @@ cudaError_t launch_visible_out(const ViewSet& vs, FwdBufs& b, uint32_t n, float*
 // a captured step can be replayed with new values.
 struct AdamScalars {
   float lr_pos, lr_rot, lr_scale, lr_color, lr_opac;
-  float beta1, beta2, eps, bc1, bc2;
+  float beta1, beta2, eps;
+  float rbc1, rbc2;  // 1 / (1 - beta^step), rounded to f32
 };
 
 struct AdamArgs {
@@ -140,23 +142,22 @@ struct AdamArgs {
 // travel as launch arguments and the call is safe to issue per step).
 cudaError_t launch_set_scalars(AdamScalars* dst, const AdamScalars& v, cudaStream_t st);
 
-// Project backward over all Gaussians for all views of the last forward.
-// mode 0 writes gradients (grad_* non-null, summed over views, scaled by
-// grad_scale) and optional per-view stats; mode 1 applies Adam in place
-// (adam non-null) and accumulates the densification statistics.
+// Project backward over all Gaussians for all views of the last forward:
+// writes the gradients (summed over views, scaled by grad_scale), optional
+// per-view stats, and optionally accumulates the densification statistics
+// view by view.
 struct ProjBwdArgs {
   float* v_tr;
   float* v_sh;
   float* v_op;
-  float* stats;  // [views][n][7] or null
-  const AdamArgs* adam;
+  float* stats;        // [views][n][7] or null
   float* densify_acc;  // [9][n] or null
   int use_visible;
   float grad_scale;
   int exact;
 };
 cudaError_t launch_project_bwd(const SplatsDev& sp, const ViewSet& vs, float cov_blur, FwdBufs& b,
-                               const ProjBwdArgs& a, const AdamArgs* adam, cudaStream_t st, int num_sms);
+                               const ProjBwdArgs& a, cudaStream_t st, int num_sms);
 
 cudaError_t launch_adam(const AdamArgs& a, const float* g_tr, const float* g_sh, const float* g_op, uint32_t n,
                         int degree, int sh_bf16, cudaStream_t st, int num_sms);

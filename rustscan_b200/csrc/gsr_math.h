@@ -37,6 +37,44 @@ GSR_HD double gfma(double a, double b, double c) { return fma(a, b, c); }
 GSR_HD float gabs(float a) { return fabsf(a); }
 GSR_HD double gabs(double a) { return fabs(a); }
 template <class F> GSR_HD F clampf(F x, F lo, F hi) { return gmin(gmax(x, lo), hi); }
+// Individually rounded float operations that no compiler may fuse into a
+// multiply-add, for the expressions whose bits decide integer outputs (the
+// blend decisions). Plain operators on the host, where the oracle is built
+// with -ffp-contract=off.
+GSR_HD float emul(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+GSR_HD float eadd(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+GSR_HD float esub(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+GSR_HD double emul(double a, double b) { return a * b; }
+GSR_HD double eadd(double a, double b) { return a + b; }
+GSR_HD double esub(double a, double b) { return a - b; }
+
+// 1/x correctly rounded (the same value as the IEEE division on the host).
+GSR_HD float grcp(float x) {
+#if defined(__CUDA_ARCH__)
+  return __frcp_rn(x);
+#else
+  return 1.0f / x;
+#endif
+}
+GSR_HD double grcp(double x) { return 1.0 / x; }
 
 GSR_HD float bits_to_float(uint32_t u) {
 #if defined(__CUDA_ARCH__)
@@ -612,21 +650,72 @@ template <class F> GSR_HD V3<F> view_dir(const Cam<F>& cam, V3<F> mean) {
 // ----------------------------------------------------------------------------
 // Per-pixel blend step (rasterize.wgsl:257-276).
 // ----------------------------------------------------------------------------
-// sigma = 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with d = mean - pixel centre.
-template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
-  return F(0.5) * (ca * dx * dx + F(2) * cb * dx * dy + cc * dy * dy);
+// sigma = 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with d = mean - pixel centre,
+// each operation rounded on its own. blend_sigma_shared takes the two
+// per-column terms t1 = a*dx*dx and t2 = 2b*dx precomputed (kernels share
+// them between the pixels of a column).
+template <class F> GSR_HD F blend_sigma_shared(F t1, F t2, F dy, F cc) {
+  return emul(F(0.5), eadd(eadd(t1, emul(t2, dy)), emul(emul(cc, dy), dy)));
 }
+template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
+  return blend_sigma_shared(emul(emul(ca, dx), dx), emul(emul(F(2), cb), dx), dy, cc);
+}
+
+// exp(x) for the blend, where x = -sigma <= 0 matters (x > 0 only occurs
+// for sigma < 0, which the contribution test rejects whatever the value):
+// the reduction and polynomial of portable_expf, with n = round(x*log2(e))
+// taken by adding 1.5*2^23 (round-to-nearest-even, exact for |x*log2e| <
+// 2^22; its integer then sits in the low mantissa bits) and the scaling by
+// 2^n done by adding n to the exponent field, exact because the result stays
+// a normal number for x >= -87.33. Same IEEE operations on host and device.
+GSR_HD float blend_expf(float x) {
+  x = fminf(x, 0.0f);
+  if (!(x > -87.3365f)) return (x != x) ? x : 0.0f;
+  const float t = eadd(emul(x, 1.44269504088896341f), 12582912.0f);
+  const float n = esub(t, 12582912.0f);
+  const int ni = (int)(float_to_bits(t) - 0x4B400000u);
+  float r = fmaf(-n, 0.693145751953125f, x);
+  r = fmaf(-n, 1.42860682030941723e-06f, r);
+  float p = 1.98412698412698413e-04f;
+  p = fmaf(p, r, 1.38888888888888889e-03f);
+  p = fmaf(p, r, 8.33333333333333333e-03f);
+  p = fmaf(p, r, 4.16666666666666667e-02f);
+  p = fmaf(p, r, 1.66666666666666667e-01f);
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
+  return bits_to_float(float_to_bits(p) + ((uint32_t)ni << 23));
+}
+GSR_HD double blend_expf(double x) { return exp(x); }
+
 // alpha = min(0.999, opac * exp(-sigma)); returns it when the Gaussian
 // contributes (sigma >= 0 and alpha >= 1/255), else -1. gauss = exp(-sigma).
 template <class F> GSR_HD F blend_alpha_of(F sigma, F opac, F& gauss) {
-  gauss = gexp(-sigma);
-  const F alpha = gmin(F(0.999), opac * gauss);
+  gauss = blend_expf(-sigma);
+  const F alpha = gmin(F(0.999), emul(opac, gauss));
   if (sigma >= F(0) && alpha >= F(1.0 / 255.0)) return alpha;
   return F(-1);
 }
 template <class F> GSR_HD F blend_alpha(F px, F py, F mx, F my, F ca, F cb, F cc, F opac, F& gauss) {
   return blend_alpha_of(blend_sigma(mx - px, my - py, ca, cb, cc), opac, gauss);
 }
+// Colour accumulation C += max(c, 0) * w as one fused multiply-add.
+template <class F> GSR_HD F blend_accum(F C, F c, F w) { return gfma(gmax(c, F(0)), w, C); }
+
+// Padded half-widths of the box around the ellipse {0.5 d^T C d <= cut}
+// (C = conic): sqrt(2 cut (C^-1)_ii), determinant in double, widened by 0.1%
+// plus 0.01 px so that float rounding can never put a pixel of the true
+// ellipse outside it. Returns false (no box) for non-positive-definite
+// conics or non-finite input.
+GSR_HD bool footprint_box(float a, float b, float c, float cut, float& rx, float& ry) {
+  const double det = (double)a * (double)c - (double)b * (double)b;
+  if (!(det > 0.0) || !(a > 0.0f) || !(c > 0.0f) || !(cut > 0.0f)) return false;
+  const double q = 2.0 * (double)cut / det;
+  rx = (float)(sqrt(q * (double)c) * 1.001 + 0.01);
+  ry = (float)(sqrt(q * (double)a) * 1.001 + 0.01);
+  return rx == rx && ry == ry && rx < 3.0e38f && ry < 3.0e38f;
+}
+
 // A Gaussian whose sigma exceeds log(255 * opac) + kRejectMargin cannot pass
 // the alpha >= 1/255 test: its exact alpha is below (1/255) * exp(-1e-3),
 // far outside the few-ulp error of the float exp and log. Kernels use this
@@ -790,10 +879,96 @@ template <class F> struct ParamGrad {
 // both terms are included and the result is the true adjoint of
 // project_gaussian + sh_to_color. coeff(k, ch) gives SH coefficients (read
 // only when exact).
+// Gradient of f(d) = sum_{k>=1} w_k b_k(d) with respect to the direction
+// d = (x, y, z), from the derivatives of the basis polynomials of sh_basis
+// (degrees 1-3 written out; degree 4 goes through dual numbers).
+template <class F> GSR_HD V3<F> sh_weighted_grad(int degree, F x, F y, F z, const F* w) {
+  V3<F> g;
+  g.x = g.y = g.z = F(0);
+  if (degree <= 0) return g;
+  if (degree >= 4) {
+    F b[25], db[25][3];
+    V3<F> d;
+    d.x = x;
+    d.y = y;
+    d.z = z;
+    sh_basis_grad<F>(degree, d, b, db);
+    for (int k = 1; k < num_sh_coeffs(degree); ++k) {
+      g.x = g.x + w[k] * db[k][0];
+      g.y = g.y + w[k] * db[k][1];
+      g.z = g.z + w[k] * db[k][2];
+    }
+    return g;
+  }
+  const F A = F(0.48860251190292);
+  g.x = -A * w[3];
+  g.y = -A * w[1];
+  g.z = A * w[2];
+  if (degree == 1) return g;
+  const F t1a = F(0.5462742152960395), c0b = F(1.092548430592079), c6 = F(0.9461746957575601);
+  // b4 = t1a 2xy, b5 = -c0b zy, b6 = c6 z^2 - c, b7 = -c0b zx, b8 = t1a (x^2 - y^2)
+  g.x = g.x + w[4] * (F(2) * t1a * y) - w[7] * (c0b * z) + w[8] * (F(2) * t1a * x);
+  g.y = g.y + w[4] * (F(2) * t1a * x) - w[5] * (c0b * z) - w[8] * (F(2) * t1a * y);
+  g.z = g.z - w[5] * (c0b * y) + w[6] * (F(2) * c6 * z) - w[7] * (c0b * x);
+  if (degree == 2) return g;
+  const F t2a = F(-0.5900435899266435), c1b = F(1.445305721320277), c0c = F(2.285228997322329);
+  const F c0c0 = F(0.4570457994644658), c12a = F(1.865881662950577), c12b = F(1.119528997770346);
+  const F t0c = -c0c * z * z + c0c0;
+  const F x2 = x * x, y2 = y * y;
+  // b9 = t2a (3x^2 y - y^3), b10 = c1b z 2xy, b11 = t0c y, b12 = z (c12a z^2 - c12b),
+  // b13 = t0c x, b14 = c1b z (x^2 - y^2), b15 = t2a (x^3 - 3 x y^2)
+  g.x = g.x + w[9] * (t2a * F(6) * x * y) + w[10] * (c1b * F(2) * y * z) + w[13] * t0c +
+        w[14] * (c1b * F(2) * x * z) + w[15] * (t2a * F(3) * (x2 - y2));
+  g.y = g.y + w[9] * (t2a * F(3) * (x2 - y2)) + w[10] * (c1b * F(2) * x * z) + w[11] * t0c -
+        w[14] * (c1b * F(2) * y * z) - w[15] * (t2a * F(6) * x * y);
+  g.z = g.z + w[10] * (c1b * F(2) * x * y) - w[11] * (F(2) * c0c * z * y) +
+        w[12] * (F(3) * c12a * z * z - c12b) - w[13] * (F(2) * c0c * z * x) + w[14] * (c1b * (x2 - y2));
+  return g;
+}
+
+// Gradient of the SH colour with respect to the mean through the view
+// direction (dir = normalize(mean - campos)): sum_k (sum_ch v_color_ch *
+// coeff_k,ch) * d b_k / d dir, chained through the normalisation. The
+// reference omits this term.
+template <class F, class Coeff>
+GSR_HD V3<F> sh_viewdir_vjp(const Cam<F>& cam, V3<F> mean, V3<F> vd, int degree, V3<F> v_color, const Coeff& coeff) {
+  V3<F> out;
+  out.x = out.y = out.z = F(0);
+  if (degree <= 0) return out;
+  const int k = num_sh_coeffs(degree);
+  F w[25];
+  w[0] = F(0);
+  for (int i = 1; i < k; ++i) w[i] = v_color.x * coeff(i, 0) + v_color.y * coeff(i, 1) + v_color.z * coeff(i, 2);
+  const V3<F> gg = sh_weighted_grad<F>(degree, vd.x, vd.y, vd.z, w);
+  const F gv[3] = {gg.x, gg.y, gg.z};
+  // d(d/|d|) = (I - u u^T) / |d| with u the unit view direction.
+  V3<F> d;
+  d.x = mean.x - cam.campos.x;
+  d.y = mean.y - cam.campos.y;
+  d.z = mean.z - cam.campos.z;
+  const F n2 = d.x * d.x + d.y * d.y + d.z * d.z;
+  if (n2 > F(1e-12)) {
+    const F inv = F(1) / gsqrt(n2);
+    const F ug = vd.x * gv[0] + vd.y * gv[1] + vd.z * gv[2];
+    out.x = (gv[0] - vd.x * ug) * inv;
+    out.y = (gv[1] - vd.y * ug) * inv;
+    out.z = (gv[2] - vd.z * ug) * inv;
+  } else {
+    const F inv = F(1) / gsqrt(F(1e-12));
+    out.x = gv[0] * inv;
+    out.y = gv[1] * inv;
+    out.z = gv[2] * inv;
+  }
+  return out;
+}
+
+// exact == false reproduces the reference approximations (see above);
+// sh_dir == false leaves out only the view-direction term even when exact
+// (callers that add sh_viewdir_vjp themselves).
 template <class F, class Coeff>
 GSR_HD ParamGrad<F> project_backward(const Cam<F>& cam, V3<F> mean, V4<F> quat_unorm, V3<F> log_scale, F raw_opac,
                                      F cov_blur, V2<F> v_xy, V3<F> v_conic, V3<F> v_color, F v_opac, int degree,
-                                     const Coeff& coeff, bool exact) {
+                                     const Coeff& coeff, bool exact, bool sh_dir = true) {
   ParamGrad<F> g;
   const V3<F> vd = view_dir(cam, mean);
   g.viewdir = vd;
@@ -842,36 +1017,11 @@ GSR_HD ParamGrad<F> project_backward(const Cam<F>& cam, V3<F> mean, V4<F> quat_u
   g.v_log_scale.z = v_scale.z * scale.z;
   g.v_quat = normalize_vjp_apply(quat_unorm, quat_to_mat3_vjp(quat, rot_scale(v_m, scale)));
   g.v_mean = mulv(transpose(cam.rot), v_mc);
-  if (exact && degree > 0) {
-    F b[25], db[25][3];
-    sh_basis_grad<F>(degree, vd, b, db);
-    const int k = num_sh_coeffs(degree);
-    F gv[3] = {F(0), F(0), F(0)};
-    const F vc[3] = {v_color.x, v_color.y, v_color.z};
-    for (int i = 1; i < k; ++i) {
-      const F w = vc[0] * coeff(i, 0) + vc[1] * coeff(i, 1) + vc[2] * coeff(i, 2);
-      gv[0] = gv[0] + w * db[i][0];
-      gv[1] = gv[1] + w * db[i][1];
-      gv[2] = gv[2] + w * db[i][2];
-    }
-    // d(d/|d|) = (I - u u^T) / |d| with u the unit view direction.
-    V3<F> d;
-    d.x = mean.x - cam.campos.x;
-    d.y = mean.y - cam.campos.y;
-    d.z = mean.z - cam.campos.z;
-    const F n2 = d.x * d.x + d.y * d.y + d.z * d.z;
-    if (n2 > F(1e-12)) {
-      const F inv = F(1) / gsqrt(n2);
-      const F ug = vd.x * gv[0] + vd.y * gv[1] + vd.z * gv[2];
-      g.v_mean.x = g.v_mean.x + (gv[0] - vd.x * ug) * inv;
-      g.v_mean.y = g.v_mean.y + (gv[1] - vd.y * ug) * inv;
-      g.v_mean.z = g.v_mean.z + (gv[2] - vd.z * ug) * inv;
-    } else {
-      const F inv = F(1) / gsqrt(F(1e-12));
-      g.v_mean.x = g.v_mean.x + gv[0] * inv;
-      g.v_mean.y = g.v_mean.y + gv[1] * inv;
-      g.v_mean.z = g.v_mean.z + gv[2] * inv;
-    }
+  if (exact && sh_dir && degree > 0) {
+    const V3<F> vm = sh_viewdir_vjp(cam, mean, vd, degree, v_color, coeff);
+    g.v_mean.x = g.v_mean.x + vm.x;
+    g.v_mean.y = g.v_mean.y + vm.y;
+    g.v_mean.z = g.v_mean.z + vm.z;
   }
   return g;
 }
@@ -885,7 +1035,7 @@ GSR_HD ParamGrad<F> project_backward(const Cam<F>& cam, V3<F> mean, V4<F> quat_u
 template <class F>
 GSR_HD void blend_step_grad(F dx, F dy, F ca, F cb, F cc, F r, F gcol, F bcol, F opac, F gauss, F alpha, F& T,
                             F S[3], const F vrgb[3], F K, bool ref_skip, SplatGrad<F>& g) {
-  const F ra = F(1) / (F(1) - alpha);
+  const F ra = grcp(F(1) - alpha);
   const F Ti = T * ra;
   const F cp[3] = {gmax(r, F(0)), gmax(gcol, F(0)), gmax(bcol, F(0))};
   const F craw[3] = {r, gcol, bcol};

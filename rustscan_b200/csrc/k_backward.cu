@@ -1,13 +1,13 @@
 // k_backward.cu — projection backward (project_backwards.wgsl:12-151) over
-// all views of the last forward, optionally fused with the bias-corrected
-// Adam update (engine/optimizer.rs:122-162) and the densification
-// statistics (engine/trainer.rs:651-728).
+// all views of the last forward, the densification statistics
+// (engine/trainer.rs:651-728) and the bias-corrected Adam update
+// (engine/optimizer.rs:122-162).
 //
-// One thread per Gaussian, views in a fixed order: the gradient of the sum
-// over views is formed in registers and written once (or consumed by Adam in
-// place, so the [N, 10+3K+1] gradient never touches memory in a training
-// step). Rows of Gaussians no view sees get zero gradients, as the reference
-// zero-fills.
+// Two passes: one thread per (view, visible Gaussian) forms that view's
+// projection adjoint into a pair record; one thread per Gaussian then sums
+// its records over the views in a fixed order and writes the gradient once.
+// Rows of Gaussians no view sees get zero gradients, as the reference
+// zero-fills. Adam is a separate element-wise pass with 16-byte accesses.
 #include <cuda_bf16.h>
 
 #include "gsr_kernels.h"
@@ -16,179 +16,320 @@ namespace gsr {
 
 namespace {
 
-struct PBArgs {
+// ---------------------------------------------------------------------------
+// Kernel A: one thread per (view, visible Gaussian). The projection adjoint
+// of that view (everything but the SH view-direction term) goes into a
+// 96-byte pair record, stored as six planes of float4 ([view][6][Vcap]) so
+// that a warp reading one part for consecutive Gaussians reads 512
+// contiguous bytes:
+//   q0 = (v_mean, v_raw_opacity)   q1 = v_quat
+//   q2 = (v_log_scale, depth)      q3 = (view direction, visible flag)
+//   q4 = (v_rgb, pixel count)      q5 = (v_xy, |v_xy| sums)
+// ---------------------------------------------------------------------------
+struct PairArgs {
   SplatsDev sp;
   ViewSet vs;
   float cov_blur;
+  FwdBufs b;
+  int exact;
+};
+
+struct NoCoeff {
+  __device__ float operator()(int, int) const { return 0.f; }
+};
+
+__global__ void __launch_bounds__(128) pair_bwd_kernel(PairArgs a) {
+  const uint32_t v = blockIdx.y;
+  const uint32_t V = a.b.vcount[v * 4 + 0];
+  const ViewDesc& vd = a.vs.views[v];
+  const Cam<float> cam = cam_from_desc<float>(vd);
+  const uint32_t* gid_of_c = slice(a.b.gid_of_c, a.b.Vcap, v);
+  const float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
+  const uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
+  float4* pair = slice(a.b.pair, a.b.Vcap * 6, v);
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < V; c += gridDim.x * blockDim.x) {
+    const uint32_t g = gid_of_c[c];
+    const float2* t2 = reinterpret_cast<const float2*>(a.sp.transforms + (size_t)g * 10);
+    const float2 t01 = t2[0], t23 = t2[1], t45 = t2[2], t67 = t2[3], t89 = t2[4];
+    const float4 q0 = sgrad[(size_t)c * 3 + 0], q1 = sgrad[(size_t)c * 3 + 1], q2 = sgrad[(size_t)c * 3 + 2];
+    const ParamGrad<float> pg = project_backward(
+        cam, V3<float>{t01.x, t01.y, t23.x}, V4<float>{t23.y, t45.x, t45.y, t67.x}, V3<float>{t67.y, t89.x, t89.y},
+        a.sp.raw_opac[g], a.cov_blur, V2<float>{q0.x, q0.y}, V3<float>{q0.z, q0.w, q1.x}, V3<float>{q1.y, q1.z, q1.w},
+        q2.x, a.sp.degree, NoCoeff(), a.exact != 0, false);
+    const size_t cap = a.b.Vcap;
+    pair[0 * cap + c] = make_float4(pg.v_mean.x, pg.v_mean.y, pg.v_mean.z, pg.v_raw_opac);
+    pair[1 * cap + c] = make_float4(pg.v_quat.x, pg.v_quat.y, pg.v_quat.z, pg.v_quat.w);
+    pair[2 * cap + c] = make_float4(pg.v_log_scale.x, pg.v_log_scale.y, pg.v_log_scale.z, pg.depth);
+    pair[3 * cap + c] = make_float4(pg.viewdir.x, pg.viewdir.y, pg.viewdir.z, vis[c] ? 1.f : 0.f);
+    pair[4 * cap + c] = make_float4(q1.y, q1.z, q1.w, q2.w);
+    pair[5 * cap + c] = make_float4(q0.x, q0.y, q2.y, q2.z);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel B: one thread per Gaussian, views in a fixed order. Sums the pair
+// records (plus the SH view-direction term, which needs the coefficients),
+// writes the per-view statistics and the densification sums, and writes the
+// summed gradient (times grad_scale) as [n][10], [n][3K], [n]. Compaction
+// runs in global-id order, so consecutive threads read consecutive pair
+// records of a view: every load is coalesced and no staging is needed.
+// ---------------------------------------------------------------------------
+struct GatherArgs {
+  SplatsDev sp;
+  ViewSet vs;
   FwdBufs b;
   float* v_tr;
   float* v_sh;
   float* v_op;
   float* stats;
-  AdamArgs adam;
-  int do_adam;
   float* acc;
   int use_visible;
   float grad_scale;
   int exact;
 };
 
-__device__ __forceinline__ float adam_one(float p, float g, float* m, float* v, float lr, const AdamScalars& a) {
-  const float m1 = *m * a.beta1 + g * (1.0f - a.beta1);
-  const float m2 = *v * a.beta2 + (g * g) * (1.0f - a.beta2);
-  *m = m1;
-  *v = m2;
-  const float mh = m1 / a.bc1, vh = m2 / a.bc2;
-  const float upd = mh / (sqrtf(vh) + a.eps);
-  return p - upd * lr;
-}
-
 __device__ __forceinline__ float to_f(float x) { return x; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
-__device__ __forceinline__ void store_sh(float* p, float x) { *p = x; }
-__device__ __forceinline__ void store_sh(__nv_bfloat16* p, float x) { *p = __float2bfloat16_rn(x); }
+
+// A block owns kGT consecutive Gaussians. Shared memory holds, per Gaussian,
+// one row of its SH values (read by the view-direction term; staged with
+// coalesced loads) that is reused for its SH gradients on the way out, plus a
+// row of transform and opacity gradients, so that every global write is
+// coalesced too.
+constexpr int kGT = 128;
+
+template <int K> struct GatherSmem {
+  static constexpr int kSh = 3 * K + 1;  // odd stride: conflict-free rows
+  static constexpr int kTr = 11;
+  static constexpr size_t kBytes = sizeof(float) * (kGT * kSh + kGT * kTr);
+};
 
 template <class SHT, int DEG>
-__global__ void __launch_bounds__(128) project_bwd_kernel(PBArgs a) {
+__global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArgs a) {
   constexpr int K = (DEG + 1) * (DEG + 1);
+  constexpr int NSH = 3 * K;
+  using L = GatherSmem<K>;
+  extern __shared__ float smem[];
+  float* s_row = smem;                 // [kGT][kSh]: SH values, then SH gradients
+  float* s_tg = smem + kGT * L::kSh;   // [kGT][kTr]: transform + opacity gradients
   const uint32_t n = a.sp.n;
+  const uint32_t nv = a.vs.n_views;
+  const float sc = a.grad_scale;
   const SHT* sh = reinterpret_cast<const SHT*>(a.sp.sh);
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
-    const float* t = a.sp.transforms + (size_t)g * 10;
-    float tp[10];
+  const bool dir_term = a.exact != 0 && DEG > 0;
+  const uint32_t r = threadIdx.x;
+  for (uint32_t g0 = blockIdx.x * kGT; g0 < n; g0 += gridDim.x * kGT) {
+    const uint32_t rows = min((uint32_t)kGT, n - g0);
+    const uint32_t g = g0 + r;
+    const bool own = r < rows;
+    __syncthreads();
+    if (dir_term) {
+      const SHT* src = sh + (size_t)g0 * NSH;
+      for (uint32_t e = r; e < rows * NSH; e += kGT) s_row[(e / NSH) * L::kSh + (e % NSH)] = to_f(src[e]);
+    }
+    __syncthreads();
+    V3<float> mean{0.f, 0.f, 0.f};
+    if (own && dir_term) {
+      const float* t = a.sp.transforms + (size_t)g * 10;
+      mean = V3<float>{t[0], t[1], t[2]};
+    }
+    const float* cf = s_row + r * L::kSh;
+    auto coeff = [&](int k, int ch) { return cf[k * 3 + ch]; };
+    float sg[NSH];
 #pragma unroll
-    for (int k = 0; k < 10; ++k) tp[k] = t[k];
-    const V3<float> mean{tp[0], tp[1], tp[2]};
-    const V4<float> quat{tp[3], tp[4], tp[5], tp[6]};
-    const V3<float> ls{tp[7], tp[8], tp[9]};
-    const float raw = a.sp.raw_opac[g];
-    const SHT* shg = sh + (size_t)g * K * 3;
-    float coef[K * 3];
-#pragma unroll
-    for (int k = 0; k < K * 3; ++k) coef[k] = to_f(shg[k]);
-    auto coeff = [&](int k, int ch) { return coef[k * 3 + ch]; };
-    float gt[10], gsh[K * 3], gop = 0.f;
+    for (int i = 0; i < NSH; ++i) sg[i] = 0.f;
+    float gt[10], gop = 0.f;
 #pragma unroll
     for (int k = 0; k < 10; ++k) gt[k] = 0.f;
+    float ac[9];
+    if (own && a.acc) {
 #pragma unroll
-    for (int k = 0; k < K * 3; ++k) gsh[k] = 0.f;
-    for (uint32_t v = 0; v < a.vs.n_views; ++v) {
-      const int32_t c = slice(a.b.c_of_gid, a.b.Ncap, v)[g];
+      for (int k = 0; k < 9; ++k) ac[k] = a.acc[k * (size_t)n + g];
+    }
+    int32_t c_next = (own && nv > 0) ? a.b.c_of_gid[g] : -1;
+    for (uint32_t v = 0; v < nv; ++v) {
+      const int32_t c = c_next;
+      if (v + 1 < nv) c_next = own ? slice(a.b.c_of_gid, a.b.Ncap, v + 1)[g] : -1;
       float st[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       float g2d = 0.f, gcol = 0.f, visf = 0.f;
       if (c >= 0) {
-        const float4* sgp = slice(a.b.sgrad, a.b.Vcap * 3, v) + (size_t)c * 3;
-        const float4 q0 = sgp[0], q1 = sgp[1], q2 = sgp[2];
-        const ViewDesc& vd = a.vs.views[v];
-        const Cam<float> cam = cam_from_desc<float>(vd);
-        const ParamGrad<float> pg =
-            project_backward(cam, mean, quat, ls, raw, a.cov_blur, V2<float>{q0.x, q0.y}, V3<float>{q0.z, q0.w, q1.x},
-                             V3<float>{q1.y, q1.z, q1.w}, q2.x, DEG, coeff, a.exact != 0);
+        const float4* P = slice(a.b.pair, a.b.Vcap * 6, v) + c;
+        const size_t cap = a.b.Vcap;
+        const float4 q0 = P[0], q1 = P[cap], q2 = P[2 * cap], q3 = P[3 * cap], q4 = P[4 * cap], q5 = P[5 * cap];
+        V3<float> vm{q0.x, q0.y, q0.z};
+        const V3<float> dir{q3.x, q3.y, q3.z};
+        if (dir_term) {
+          const Cam<float> cam = cam_from_desc<float>(a.vs.views[v]);
+          const V3<float> d = sh_viewdir_vjp(cam, mean, dir, DEG, V3<float>{q4.x, q4.y, q4.z}, coeff);
+          vm.x += d.x;
+          vm.y += d.y;
+          vm.z += d.z;
+        }
+        gt[0] += vm.x;
+        gt[1] += vm.y;
+        gt[2] += vm.z;
+        gt[3] += q1.x;
+        gt[4] += q1.y;
+        gt[5] += q1.z;
+        gt[6] += q1.w;
+        gt[7] += q2.x;
+        gt[8] += q2.y;
+        gt[9] += q2.z;
+        gop += q0.w;
         float bas[25];
-        sh_basis<float>(DEG, pg.viewdir.x, pg.viewdir.y, pg.viewdir.z, bas);
-        const float vg[10] = {pg.v_mean.x, pg.v_mean.y, pg.v_mean.z, pg.v_quat.x, pg.v_quat.y,
-                              pg.v_quat.z, pg.v_quat.w, pg.v_log_scale.x, pg.v_log_scale.y, pg.v_log_scale.z};
-#pragma unroll
-        for (int k = 0; k < 10; ++k) gt[k] = gt[k] + vg[k];
-        gop = gop + pg.v_raw_opac;
+        sh_basis<float>(DEG, dir.x, dir.y, dir.z, bas);
         float csum = 0.f;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const float s0 = bas[k] * q1.y, s1 = bas[k] * q1.z, s2 = bas[k] * q1.w;
-          gsh[k * 3 + 0] = gsh[k * 3 + 0] + s0;
-          gsh[k * 3 + 1] = gsh[k * 3 + 1] + s1;
-          gsh[k * 3 + 2] = gsh[k * 3 + 2] + s2;
-          csum = csum + (fabsf(s0) + fabsf(s1) + fabsf(s2)) / 3.0f;
+          const float s0 = bas[k] * q4.x, s1 = bas[k] * q4.y, s2 = bas[k] * q4.z;
+          sg[k * 3 + 0] += s0;
+          sg[k * 3 + 1] += s1;
+          sg[k * 3 + 2] += s2;
+          csum += (fabsf(s0) + fabsf(s1) + fabsf(s2)) / 3.0f;
         }
+        // Densification quantities of this view (engine/trainer.rs:660-727).
+        g2d = (fabsf(vm.x) + fabsf(vm.y) + fabsf(vm.z)) / 3.0f;
         gcol = csum / (float)K;
-        g2d = (fabsf(vg[0]) + fabsf(vg[1]) + fabsf(vg[2])) / 3.0f;
         // project_backwards.wgsl:192-205, 274-277.
-        st[0] = q0.x;
-        st[1] = q0.y;
-        st[2] = q2.y;
-        st[3] = q2.z;
-        const float abs_score = sqrtf(q2.y * q2.y + q2.z * q2.z);
-        st[4] = q2.w * abs_score;
-        st[5] = q2.w;
-        st[6] = q2.w * pg.depth;
-        visf = slice(a.b.visible_c, a.b.Vcap, v)[c] ? 1.f : 0.f;
+        st[0] = q5.x;
+        st[1] = q5.y;
+        st[2] = q5.z;
+        st[3] = q5.w;
+        st[4] = q4.w * sqrtf(q5.z * q5.z + q5.w * q5.w);
+        st[5] = q4.w;
+        st[6] = q4.w * q2.w;
+        visf = q3.w;
       }
-      if (a.stats) {
+      if (own && a.stats) {
         float* so = a.stats + ((size_t)v * n + g) * 7;
 #pragma unroll
         for (int k = 0; k < 7; ++k) so[k] = st[k];
       }
       if (a.acc) {
-        // engine/trainer.rs:660-727 for this view.
-        float* acc = a.acc;
-        acc[0 * (size_t)n + g] += g2d;
-        acc[1 * (size_t)n + g] += sqrtf(st[0] * st[0] + st[1] * st[1]);
-        acc[2 * (size_t)n + g] += sqrtf(st[2] * st[2] + st[3] * st[3]);
-        acc[3 * (size_t)n + g] += st[4];
-        acc[4 * (size_t)n + g] += st[5];
-        acc[5 * (size_t)n + g] += st[6];
-        acc[6 * (size_t)n + g] += gcol;
-        acc[7 * (size_t)n + g] += 1.0f;
-        acc[8 * (size_t)n + g] += a.use_visible ? visf : 1.0f;
+        // One view at a time, in view order, as a per-view accumulation does.
+        ac[0] += g2d;
+        ac[1] += sqrtf(st[0] * st[0] + st[1] * st[1]);
+        ac[2] += sqrtf(st[2] * st[2] + st[3] * st[3]);
+        ac[3] += st[4];
+        ac[4] += st[5];
+        ac[5] += st[6];
+        ac[6] += gcol;
+        ac[7] += 1.0f;
+        ac[8] += a.use_visible ? visf : 1.0f;
       }
     }
-    const float sc = a.grad_scale;
-    if (!a.do_adam) {
-      float* o = a.v_tr + (size_t)g * 10;
+    if (own && a.acc) {
 #pragma unroll
-      for (int k = 0; k < 10; ++k) o[k] = gt[k] * sc;
-      float* os = a.v_sh + (size_t)g * K * 3;
-#pragma unroll
-      for (int k = 0; k < K * 3; ++k) os[k] = gsh[k] * sc;
-      a.v_op[g] = gop * sc;
-    } else {
-      const AdamArgs& ad = a.adam;
-      const AdamScalars sc_ = *ad.scal;
-      float* pt = ad.transforms + (size_t)g * 10;
-      float* mt = ad.m_tr + (size_t)g * 10;
-      float* vt = ad.v_tr + (size_t)g * 10;
-#pragma unroll
-      for (int k = 0; k < 10; ++k) {
-        const float lr = k < 3 ? sc_.lr_pos : (k < 7 ? sc_.lr_rot : sc_.lr_scale);
-        pt[k] = adam_one(tp[k], gt[k] * sc, mt + k, vt + k, lr, sc_);
-      }
-      SHT* ps = reinterpret_cast<SHT*>(ad.sh) + (size_t)g * K * 3;
-      float* ms = ad.m_sh + (size_t)g * K * 3;
-      float* vs = ad.v_sh + (size_t)g * K * 3;
-#pragma unroll
-      for (int k = 0; k < K * 3; ++k)
-        store_sh(ps + k, adam_one(coef[k], gsh[k] * sc, ms + k, vs + k, sc_.lr_color, sc_));
-      ad.raw_opac[g] = adam_one(raw, gop * sc, ad.m_op + g, ad.v_op + g, sc_.lr_opac, sc_);
+      for (int k = 0; k < 9; ++k) a.acc[k * (size_t)n + g] = ac[k];
     }
+    __syncthreads();  // every thread is done with the SH values in s_row
+    float* tg = s_tg + r * L::kTr;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) tg[k] = gt[k] * sc;
+    tg[10] = gop * sc;
+    float* sgr = s_row + r * L::kSh;
+#pragma unroll
+    for (int i = 0; i < NSH; ++i) sgr[i] = sg[i] * sc;
+    __syncthreads();
+    float* vt = a.v_tr + (size_t)g0 * 10;
+    for (uint32_t e = r; e < rows * 10; e += kGT) vt[e] = s_tg[(e / 10) * L::kTr + (e % 10)];
+    float* vs = a.v_sh + (size_t)g0 * NSH;
+    for (uint32_t e = r; e < rows * NSH; e += kGT) vs[e] = s_row[(e / NSH) * L::kSh + (e % NSH)];
+    if (own) a.v_op[g] = tg[10];
   }
+}
+
+template <class SHT, int DEG> void launch_gather(int blocks, cudaStream_t st, const GatherArgs& a) {
+  constexpr int K = (DEG + 1) * (DEG + 1);
+  const size_t bytes = GatherSmem<K>::kBytes;
+  cudaFuncSetAttribute(gather_kernel<SHT, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  gather_kernel<SHT, DEG><<<blocks, kGT, bytes, st>>>(a);
 }
 
 template <class SHT>
-void dispatch_pb(int degree, int blocks, cudaStream_t st, const PBArgs& a) {
+void dispatch_gather(int degree, int blocks, cudaStream_t st, const GatherArgs& a) {
   switch (degree) {
-    case 0: project_bwd_kernel<SHT, 0><<<blocks, 128, 0, st>>>(a); break;
-    case 1: project_bwd_kernel<SHT, 1><<<blocks, 128, 0, st>>>(a); break;
-    case 2: project_bwd_kernel<SHT, 2><<<blocks, 128, 0, st>>>(a); break;
-    case 3: project_bwd_kernel<SHT, 3><<<blocks, 128, 0, st>>>(a); break;
-    default: project_bwd_kernel<SHT, 4><<<blocks, 128, 0, st>>>(a); break;
+    case 0: launch_gather<SHT, 0>(blocks, st, a); break;
+    case 1: launch_gather<SHT, 1>(blocks, st, a); break;
+    case 2: launch_gather<SHT, 2>(blocks, st, a); break;
+    case 3: launch_gather<SHT, 3>(blocks, st, a); break;
+    default: launch_gather<SHT, 4>(blocks, st, a); break;
   }
 }
 
-// Standalone Adam over one group: group 0 transforms (columns: 3 position,
-// 4 rotation, 3 scale), 1 SH coefficients, 2 opacities.
+// engine/optimizer.rs:141-161 with the bias corrections applied as
+// multiplications by their f32 reciprocals; every operation rounded on its
+// own (the file builds with multiply-add contraction; Adam must match the
+// oracle bit for bit).
+__device__ __forceinline__ float adam_one(float p, float g, float& m, float& v, float lr, const AdamScalars& a) {
+  const float m1 = eadd(emul(m, a.beta1), emul(g, esub(1.0f, a.beta1)));
+  const float m2 = eadd(emul(v, a.beta2), emul(emul(g, g), esub(1.0f, a.beta2)));
+  m = m1;
+  v = m2;
+  const float mh = emul(m1, a.rbc1), vh = emul(m2, a.rbc2);
+  const float upd = __fdiv_rn(mh, eadd(__fsqrt_rn(vh), a.eps));
+  return esub(p, emul(upd, lr));
+}
+
+__device__ __forceinline__ float group_lr(const AdamScalars& a, int group, uint32_t col) {
+  if (group == 0) return col < 3 ? a.lr_pos : (col < 7 ? a.lr_rot : a.lr_scale);
+  return group == 1 ? a.lr_color : a.lr_opac;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ld4(const __nv_bfloat16* p) {
+  const uint2 u = *reinterpret_cast<const uint2*>(p);
+  const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+  const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ void st4(float* p, float4 x) { *reinterpret_cast<float4*>(p) = x; }
+__device__ __forceinline__ void st4(__nv_bfloat16* p, float4 x) {
+  __nv_bfloat162 lo, hi;
+  lo.x = __float2bfloat16_rn(x.x);
+  lo.y = __float2bfloat16_rn(x.y);
+  hi.x = __float2bfloat16_rn(x.z);
+  hi.y = __float2bfloat16_rn(x.w);
+  uint2 u;
+  u.x = *reinterpret_cast<uint32_t*>(&lo);
+  u.y = *reinterpret_cast<uint32_t*>(&hi);
+  *reinterpret_cast<uint2*>(p) = u;
+}
+__device__ __forceinline__ void store_sh(float* p, float x) { *p = x; }
+__device__ __forceinline__ void store_sh(__nv_bfloat16* p, float x) { *p = __float2bfloat16_rn(x); }
+
+// Element-wise Adam over one parameter group (0 transforms: columns 3
+// position, 4 rotation, 3 scale; 1 SH coefficients; 2 opacities). Four
+// elements per thread with 16-byte loads and stores when every array is
+// aligned for them (vec), the remainder one by one.
 template <class PT>
-__global__ void adam_kernel(PT* p, const float* g, float* m, float* v, uint64_t n, int group,
-                            const AdamScalars* scal) {
+__global__ void __launch_bounds__(256) adam_kernel(PT* p, const float* g, float* m, float* v, uint64_t n, int group,
+                                                   int vec, const AdamScalars* scal) {
   const AdamScalars a = *scal;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    float lr;
-    if (group == 0) {
-      const int col = (int)(i % 10u);
-      lr = col < 3 ? a.lr_pos : (col < 7 ? a.lr_rot : a.lr_scale);
-    } else {
-      lr = group == 1 ? a.lr_color : a.lr_opac;
-    }
-    store_sh(p + i, adam_one(to_f(p[i]), g[i], m + i, v + i, lr, a));
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nq = vec ? n / 4 : 0;
+  for (uint64_t q = t0; q < nq; q += stride) {
+    const uint64_t i = q * 4;
+    float4 P = ld4(p + i);
+    const float4 G = ld4(g + i);
+    float4 M = ld4(m + i), Vv = ld4(v + i);
+    uint32_t col = group == 0 ? (uint32_t)(i % 10u) : 0u;
+    auto step = [&](float& pp, float gg, float& mm, float& vv) {
+      pp = adam_one(pp, gg, mm, vv, group_lr(a, group, col), a);
+      if (++col == 10u) col = 0u;
+    };
+    step(P.x, G.x, M.x, Vv.x);
+    step(P.y, G.y, M.y, Vv.y);
+    step(P.z, G.z, M.z, Vv.z);
+    step(P.w, G.w, M.w, Vv.w);
+    st4(p + i, P);
+    st4(m + i, M);
+    st4(v + i, Vv);
+  }
+  for (uint64_t i = nq * 4 + t0; i < n; i += stride) {
+    const uint32_t col = group == 0 ? (uint32_t)(i % 10u) : 0u;
+    store_sh(p + i, adam_one(to_f(p[i]), g[i], m[i], v[i], group_lr(a, group, col), a));
   }
 }
 
@@ -226,46 +367,66 @@ cudaError_t launch_set_scalars(AdamScalars* dst, const AdamScalars& v, cudaStrea
 }
 
 cudaError_t launch_project_bwd(const SplatsDev& sp, const ViewSet& vs, float cov_blur, FwdBufs& b,
-                               const ProjBwdArgs& pa, const AdamArgs* adam, cudaStream_t st, int num_sms) {
+                               const ProjBwdArgs& pa, cudaStream_t st, int num_sms) {
   if (sp.n == 0) return cudaSuccess;
-  PBArgs a{};
+  PairArgs pr{};
+  pr.sp = sp;
+  pr.vs = vs;
+  pr.cov_blur = cov_blur;
+  pr.b = b;
+  pr.exact = pa.exact;
+  int px = num_sms * 16 / (int)vs.n_views;
+  if (px < 1) px = 1;
+  pair_bwd_kernel<<<dim3(px, vs.n_views), 128, 0, st>>>(pr);
+  GatherArgs a{};
   a.sp = sp;
   a.vs = vs;
-  a.cov_blur = cov_blur;
   a.b = b;
   a.v_tr = pa.v_tr;
   a.v_sh = pa.v_sh;
   a.v_op = pa.v_op;
   a.stats = pa.stats;
-  a.do_adam = adam != nullptr;
-  if (adam) a.adam = *adam;
   a.acc = pa.densify_acc;
   a.use_visible = pa.use_visible;
   a.grad_scale = pa.grad_scale;
   a.exact = pa.exact;
-  int blocks = (int)((sp.n + 127) / 128);
-  const int cap = num_sms * 16;
+  int blocks = (int)((sp.n + kGT - 1) / kGT);
+  const int cap = num_sms * 8;
   if (blocks > cap) blocks = cap;
   if (sp.sh_bf16)
-    dispatch_pb<__nv_bfloat16>(sp.degree, blocks, st, a);
+    dispatch_gather<__nv_bfloat16>(sp.degree, blocks, st, a);
   else
-    dispatch_pb<float>(sp.degree, blocks, st, a);
+    dispatch_gather<float>(sp.degree, blocks, st, a);
   return cudaGetLastError();
 }
+
+namespace {
+bool aligned(const void* p, uintptr_t to) { return (reinterpret_cast<uintptr_t>(p) & (to - 1)) == 0; }
+
+template <class PT>
+void adam_group(PT* p, const float* g, float* m, float* v, uint64_t n, int group, const AdamScalars* scal,
+                cudaStream_t st, int num_sms) {
+  if (n == 0) return;
+  const int vec = aligned(p, 4 * sizeof(PT)) && aligned(g, 16) && aligned(m, 16) && aligned(v, 16);
+  const uint64_t units = vec ? (n + 3) / 4 : n;
+  uint64_t blocks = (units + 255) / 256;
+  const uint64_t cap = (uint64_t)num_sms * 8;
+  if (blocks > cap) blocks = cap;
+  adam_kernel<PT><<<(unsigned)blocks, 256, 0, st>>>(p, g, m, v, n, group, vec, scal);
+}
+}  // namespace
 
 cudaError_t launch_adam(const AdamArgs& a, const float* g_tr, const float* g_sh, const float* g_op, uint32_t n,
                         int degree, int sh_bf16, cudaStream_t st, int num_sms) {
   if (n == 0) return cudaSuccess;
-  const int K = (degree + 1) * (degree + 1);
-  const int blocks = num_sms * 8;
-  adam_kernel<float><<<blocks, 256, 0, st>>>(a.transforms, g_tr, a.m_tr, a.v_tr, (uint64_t)n * 10, 0, a.scal);
+  const uint64_t nsh = (uint64_t)n * (degree + 1) * (degree + 1) * 3;
+  adam_group<float>(a.transforms, g_tr, a.m_tr, a.v_tr, (uint64_t)n * 10, 0, a.scal, st, num_sms);
   if (sh_bf16)
-    adam_kernel<__nv_bfloat16><<<blocks, 256, 0, st>>>(reinterpret_cast<__nv_bfloat16*>(a.sh), g_sh, a.m_sh, a.v_sh,
-                                                       (uint64_t)n * K * 3, 1, a.scal);
+    adam_group<__nv_bfloat16>(reinterpret_cast<__nv_bfloat16*>(a.sh), g_sh, a.m_sh, a.v_sh, nsh, 1, a.scal, st,
+                              num_sms);
   else
-    adam_kernel<float><<<blocks, 256, 0, st>>>(reinterpret_cast<float*>(a.sh), g_sh, a.m_sh, a.v_sh,
-                                               (uint64_t)n * K * 3, 1, a.scal);
-  adam_kernel<float><<<blocks, 256, 0, st>>>(a.raw_opac, g_op, a.m_op, a.v_op, n, 2, a.scal);
+    adam_group<float>(reinterpret_cast<float*>(a.sh), g_sh, a.m_sh, a.v_sh, nsh, 1, a.scal, st, num_sms);
+  adam_group<float>(a.raw_opac, g_op, a.m_op, a.v_op, n, 2, a.scal, st, num_sms);
   return cudaGetLastError();
 }
 

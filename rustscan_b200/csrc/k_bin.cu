@@ -33,7 +33,8 @@ __global__ void __launch_bounds__(256) emit_kernel(ViewSet vs, FwdBufs b, int de
   const TileShape ts{vs.tile_w, vs.tile_h};
   const uint32_t* perm = slice(b.perm, b.Vcap, v);
   const uint32_t* off = slice(b.offset, b.Vcap, v);
-  const float4* rec = slice(b.rec, b.Vcap * 3, v);
+  float4* rec_w = slice(b.rec, b.Vcap * 3, v);
+  const float4* rec = rec_w;
   uint32_t* keys = slice(b.isect_key_raw, b.Icap, v);
   uint32_t* vals = slice(b.isect_val_raw, b.Icap, v);
   uint32_t* emit_c = det ? slice(b.inv_perm, b.Icap, v) : nullptr;
@@ -62,6 +63,14 @@ __global__ void __launch_bounds__(256) emit_kernel(ViewSet vs, FwdBufs b, int de
           }
           ++o;
         }
+    // The tile box is no longer needed: the record's last two slots now
+    // carry the footprint half-widths the rasterizer culls warp blocks with
+    // (negative: no box, never cull).
+    float rx = -1.f, ry = -1.f;
+    if (!footprint_box(conic.x, conic.y, conic.z, thr + kRejectMargin, rx, ry)) rx = ry = -1.f;
+    float4* rw = rec_w + (size_t)c * 3 + 2;
+    rw->z = rx;
+    rw->w = ry;
   }
 }
 

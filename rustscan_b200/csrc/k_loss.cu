@@ -211,21 +211,36 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
   }
 }
 
-__global__ void loss_reduce_kernel(LossArgs a, uint32_t n_views, float* loss) {
+// One block per view: strided partial sums in double, then a fixed-order
+// tree over the block (deterministic).
+__global__ void __launch_bounds__(256) loss_reduce_kernel(LossArgs a, uint32_t n_views, float* loss) {
+  __shared__ double s_ss[256], s_l1[256];
   const uint32_t v = blockIdx.x;
-  if (threadIdx.x != 0 || v >= n_views) return;
+  if (v >= n_views) return;
   const ViewDesc& vd = a.views[v];
   const int W = (int)vd.w, H = (int)vd.h;
   const int tiles = ((W + LTX - 1) / LTX) * ((H + LTY - 1) / LTY);
   double ss = 0.0, l1 = 0.0;
-  for (int ch = 0; ch < 3; ++ch)
-    for (int t = 0; t < tiles; ++t) {
-      const float* pp = a.partial + (((size_t)v * 3 + ch) * a.tiles_cap + t) * 2;
-      ss += pp[0];
-      l1 += pp[1];
+  for (int i = threadIdx.x; i < 3 * tiles; i += blockDim.x) {
+    const int ch = i / tiles, t = i % tiles;
+    const float* pp = a.partial + (((size_t)v * 3 + ch) * a.tiles_cap + t) * 2;
+    ss += pp[0];
+    l1 += pp[1];
+  }
+  s_ss[threadIdx.x] = ss;
+  s_l1[threadIdx.x] = l1;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      s_ss[threadIdx.x] += s_ss[threadIdx.x + o];
+      s_l1[threadIdx.x] += s_l1[threadIdx.x + o];
     }
-  const double M = 3.0 * (double)W * (double)H;
-  loss[v] = (float)((double)a.l1_w * (l1 / M) + (double)a.ssim_w * (1.0 - ss / M));
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double M = 3.0 * (double)W * (double)H;
+    loss[v] = (float)((double)a.l1_w * (s_l1[0] / M) + (double)a.ssim_w * (1.0 - s_ss[0] / M));
+  }
 }
 
 }  // namespace
@@ -271,7 +286,7 @@ cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const flo
   dim3 grid(tmax, 3, vs.n_views);
   ssim_fwd_kernel<<<grid, 256, 0, st>>>(a);
   ssim_bwd_kernel<<<grid, 256, 0, st>>>(a);
-  loss_reduce_kernel<<<vs.n_views, 32, 0, st>>>(a, vs.n_views, loss);
+  loss_reduce_kernel<<<vs.n_views, 256, 0, st>>>(a, vs.n_views, loss);
   return cudaGetLastError();
 }
 

@@ -70,3 +70,30 @@ def assert_grad_close(a, b, rtol=1e-4, floor_frac=1e-3, what=""):
     e = rel_err(a, b, floor_frac)
     worst = float(e.max(initial=0.0))
     assert worst <= rtol, f"{what}: max rel err {worst:.3e} > {rtol} (at {np.unravel_index(int(e.argmax()), e.shape)})"
+
+
+def assert_grad_parity(g, r32, r64, rtol=1e-4, floor_frac=1e-3, what=""):
+    """Gradient parity against the oracle pair (FP32 and FP64 instantiations).
+
+    1. Norm-wise: ||g - r32|| / ||r32|| <= rtol (the relative error of the
+       gradient vector, 1e-4).
+    2. Element-wise, anchored on the FP64 truth: every element is within
+       rtol of r64 (floor: floor_frac * max|r64|), or no further from r64
+       than twice the FP32 oracle's own error there. Elements whose value
+       cancels in float (where two correct FP32 roundings legitimately differ
+       by more than 1e-4) are held to the FP32 oracle's accuracy.
+    """
+    g = np.asarray(g, np.float64)
+    r32 = np.asarray(r32, np.float64)
+    r64 = np.asarray(r64, np.float64)
+    nrm = float(np.linalg.norm(r32))
+    if nrm > 0:
+        ne = float(np.linalg.norm(g - r32)) / nrm
+        assert ne <= rtol, f"{what}: norm-wise rel err {ne:.3e} > {rtol}"
+    floor = max(floor_frac * float(np.abs(r64).max(initial=0.0)), 1e-30)
+    allow = np.maximum(rtol * np.maximum(np.abs(r64), floor), 2.0 * np.abs(r32 - r64))
+    bad = np.abs(g - r64) > allow
+    if bad.any():
+        i = np.unravel_index(int(np.argmax(np.abs(g - r64) / allow)), g.shape)
+        raise AssertionError(f"{what}: {int(bad.sum())} elements outside tolerance; worst at {i}: gpu {g[i]:.8g} "
+                             f"fp32 oracle {r32[i]:.8g} fp64 oracle {r64[i]:.8g}")
