@@ -286,6 +286,7 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   GSR_CUDA(c, radix_sort_pairs(b.depth_key, nullptr, b.depth_sorted, b.perm, b.key_tmp, b.val_tmp, b.Vcap, n_views,
                                b.vcount, 4, 0, b.Vcap, 31, c->s, st));
   prof_mark(c, kStOffsets, st);
+  GSR_CUDA(c, launch_count(vs, b, c->s, st));
   GSR_CUDA(c, launch_offsets(vs, b, c->s, st));
   prof_mark(c, kStEmit, st);
   GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));

@@ -98,6 +98,8 @@ cudaError_t inclusive_scan_u32_scratch(const uint32_t* in, uint32_t* out, uint32
 // Per view: offset[r] = exclusive scan of count[perm[r]], sets vcount[1..2].
 cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 
+// Per-view tile counts of the compact records (count[c], gid order).
+cudaError_t launch_count(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
 cudaError_t launch_remap(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_ranges(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);

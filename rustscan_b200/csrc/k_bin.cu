@@ -2,12 +2,11 @@
 // (map_gaussian_to_intersects.wgsl), tile ranges (get_tile_offsets.wgsl),
 // the visibility export and the deterministic-mode gradient reduction.
 //
-// Emission walks Gaussians in depth order and writes, for every tile that
-// passes the contribution test, the tile id as key and the compact index as
-// value at the Gaussian's scanned offset. The test reads the exact float
-// values the counting pass used (stored in the projected record), so the
-// emitted set always matches the counts (the reference recomputes the extent
-// from the inverted conic here, which can disagree with its count pass).
+// Counting (the per-Gaussian tile count of project_forward.wgsl:79-91) and
+// emission both run the contribution test on the exact float values stored
+// in the projected record, so the emitted set always matches the counts (the
+// reference recomputes the extent from the inverted conic at emission, which
+// can disagree with its count pass).
 #include <cstring>
 
 #include "gsr_kernels.h"
@@ -16,17 +15,34 @@ namespace gsr {
 
 namespace {
 
-__device__ __forceinline__ TileBox unpack_box(float4 r2) {
-  const uint32_t bx = __float_as_uint(r2.z), by = __float_as_uint(r2.w);
-  TileBox b;
-  b.x0 = bx & 0xffffu;
-  b.x1 = bx >> 16;
-  b.y0 = by & 0xffffu;
-  b.y1 = by >> 16;
-  return b;
-}
+// Warp-cooperative tile walk. The 32 Gaussians of a warp have boxes of very
+// different sizes (one tile to thousands), so a loop per thread would leave
+// most lanes idle. The warp flattens its Gaussians' boxes into one item list
+// (lane-major, row-major within a box: the emission order) and every pass
+// tests 32 consecutive items, one per lane. Passing items are ranked within
+// their Gaussian with ballots, so each Gaussian's tiles keep their row-major
+// order and the output is the same as a per-Gaussian loop.
+struct WalkWarp {
+  uint32_t incl[32], ex[32];  // inclusive / exclusive prefix of box sizes
+  uint32_t x0[32], y0[32], w[32];
+  float mx[32], my[32], ca[32], cb[32], cc[32], thr[32];
+  uint32_t run[32];  // passing tiles found so far, per Gaussian
+  uint32_t off[32];  // emission offset, per Gaussian
+  uint32_t cid[32];  // compact index, per Gaussian
+};
 
-__global__ void __launch_bounds__(256) emit_kernel(ViewSet vs, FwdBufs b, int det) {
+constexpr int kWalkThreads = 256;
+constexpr int kWalkWarps = kWalkThreads / 32;
+
+// EMIT = false: count the passing tiles of every compact index (gid order).
+// EMIT = true: walk the Gaussians in depth order and write, for every
+// passing tile, the tile id as key and the compact index as value at the
+// Gaussian's scanned offset; then replace the record's tile box with the
+// footprint half-widths the rasterizer culls warp blocks with (negative: no
+// box, never cull).
+template <bool EMIT>
+__global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, FwdBufs b, int det) {
+  __shared__ WalkWarp s_w[kWalkWarps];
   const uint32_t v = blockIdx.y;
   const uint32_t V = b.vcount[v * 4 + 0];
   const ViewDesc& vd = vs.views[v];
@@ -35,42 +51,121 @@ __global__ void __launch_bounds__(256) emit_kernel(ViewSet vs, FwdBufs b, int de
   const uint32_t* off = slice(b.offset, b.Vcap, v);
   float4* rec_w = slice(b.rec, b.Vcap * 3, v);
   const float4* rec = rec_w;
+  uint32_t* count = slice(b.count, b.Vcap, v);
   uint32_t* keys = slice(b.isect_key_raw, b.Icap, v);
   uint32_t* vals = slice(b.isect_val_raw, b.Icap, v);
   uint32_t* emit_c = det ? slice(b.inv_perm, b.Icap, v) : nullptr;
   const uint64_t cap = b.Icap;
-  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < V; r += gridDim.x * blockDim.x) {
-    const uint32_t c = perm[r];
-    uint64_t o = off[r];
-    const float4 r0 = rec[(size_t)c * 3 + 0];
-    const float4 r1 = rec[(size_t)c * 3 + 1];
-    const float4 r2 = rec[(size_t)c * 3 + 2];
-    const V2<float> mean{r0.x, r0.y};
-    const V3<float> conic{r0.z, r0.w, r1.x};
-    const float thr = r2.y;
-    const TileBox box = unpack_box(r2);
-    for (uint32_t ty = box.y0; ty < box.y1; ++ty)
-      for (uint32_t tx = box.x0; tx < box.x1; ++tx)
-        if (will_primitive_contribute(tx, ty, ts, mean, conic, thr)) {
-          if (o < cap) {
-            keys[o] = tx + ty * vd.tiles_x;
-            if (det) {
-              vals[o] = (uint32_t)o;
-              emit_c[o] = c;
-            } else {
-              vals[o] = c;
-            }
-          }
-          ++o;
+  const uint32_t lane = threadIdx.x & 31u;
+  WalkWarp& S = s_w[threadIdx.x >> 5];
+  const uint32_t stride = gridDim.x * kWalkWarps * 32u;
+  for (uint32_t base = (blockIdx.x * kWalkWarps + (threadIdx.x >> 5)) * 32u; base < V; base += stride) {
+    const uint32_t r = base + lane;
+    uint32_t nb = 0u, c = 0u, x0 = 0u, y0 = 0u, w = 0u, o0 = 0u;
+    V2<float> mean{0.f, 0.f};
+    V3<float> conic{0.f, 0.f, 0.f};
+    float thr = 0.f;
+    if (r < V) {
+      c = EMIT ? perm[r] : r;
+      const float4 r0 = rec[(size_t)c * 3 + 0];
+      const float4 r1 = rec[(size_t)c * 3 + 1];
+      const float4 r2 = rec[(size_t)c * 3 + 2];
+      mean = V2<float>{r0.x, r0.y};
+      conic = V3<float>{r0.z, r0.w, r1.x};
+      thr = r2.y;
+      const uint32_t bx = __float_as_uint(r2.z), by = __float_as_uint(r2.w);
+      x0 = bx & 0xffffu;
+      y0 = by & 0xffffu;
+      const uint32_t x1 = bx >> 16, y1 = by >> 16;
+      w = x1 > x0 ? x1 - x0 : 0u;
+      nb = w * (y1 > y0 ? y1 - y0 : 0u);
+      if (EMIT) o0 = off[r];
+    }
+    uint32_t incl = nb;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= (uint32_t)d) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();  // the previous round's readers of S are done
+    S.incl[lane] = incl;
+    S.ex[lane] = incl - nb;
+    S.x0[lane] = x0;
+    S.y0[lane] = y0;
+    S.w[lane] = w;
+    S.mx[lane] = mean.x;
+    S.my[lane] = mean.y;
+    S.ca[lane] = conic.x;
+    S.cb[lane] = conic.y;
+    S.cc[lane] = conic.z;
+    S.thr[lane] = thr;
+    S.run[lane] = 0u;
+    S.off[lane] = o0;
+    S.cid[lane] = c;
+    __syncwarp();
+    for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+      const uint32_t t = t0 + lane;
+      const bool live = t < total;
+      uint32_t owner = 0u, tx = 0u, ty = 0u;
+      bool pass = false;
+      if (live) {
+        // The first Gaussian whose inclusive prefix exceeds t (exists: t < total).
+        uint32_t lo = 0u, hi = 31u;
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (S.incl[mid] > t)
+            hi = mid;
+          else
+            lo = mid + 1u;
         }
-    // The tile box is no longer needed: the record's last two slots now
-    // carry the footprint half-widths the rasterizer culls warp blocks with
-    // (negative: no box, never cull).
-    float rx = -1.f, ry = -1.f;
-    if (!footprint_box(conic.x, conic.y, conic.z, thr + kRejectMargin, rx, ry)) rx = ry = -1.f;
-    float4* rw = rec_w + (size_t)c * 3 + 2;
-    rw->z = rx;
-    rw->w = ry;
+        owner = lo;
+        const uint32_t local = t - S.ex[owner];
+        const uint32_t ow = S.w[owner];
+        const uint32_t ry = local / ow;
+        tx = S.x0[owner] + (local - ry * ow);
+        ty = S.y0[owner] + ry;
+        pass = will_primitive_contribute(tx, ty, ts, V2<float>{S.mx[owner], S.my[owner]},
+                                         V3<float>{S.ca[owner], S.cb[owner], S.cc[owner]}, S.thr[owner]);
+      }
+      const uint32_t pm = __ballot_sync(0xffffffffu, pass);
+      const uint32_t prev = __shfl_up_sync(0xffffffffu, owner, 1);
+      const bool start = live && (lane == 0u || prev != owner);
+      const uint32_t sm = __ballot_sync(0xffffffffu, start);
+      if (EMIT && pass) {
+        const uint32_t first = 31u - (uint32_t)__clz(sm & ((2u << lane) - 1u));
+        const uint32_t before = pm & ((1u << lane) - 1u) & ~((1u << first) - 1u);
+        const uint64_t o = (uint64_t)S.off[owner] + S.run[owner] + (uint32_t)__popc(before);
+        if (o < cap) {
+          keys[o] = tx + ty * vd.tiles_x;
+          if (det) {
+            vals[o] = (uint32_t)o;
+            emit_c[o] = S.cid[owner];
+          } else {
+            vals[o] = S.cid[owner];
+          }
+        }
+      }
+      __syncwarp();
+      if (start) {
+        const uint32_t later = sm & ~((2u << lane) - 1u);
+        const uint32_t seg_hi = later ? ((1u << (__ffs(later) - 1)) - 1u) : 0xffffffffu;
+        S.run[owner] += (uint32_t)__popc(pm & seg_hi & ~((1u << lane) - 1u));
+      }
+      __syncwarp();
+    }
+    if (r < V) {
+      if (!EMIT) {
+        count[c] = S.run[lane];
+      } else {
+        float rx = -1.f, ry = -1.f;
+        if (!footprint_box(conic.x, conic.y, conic.z, thr + kRejectMargin, rx, ry)) rx = ry = -1.f;
+        float4* rw = rec_w + (size_t)c * 3 + 2;
+        rw->z = rx;
+        rw->w = ry;
+      }
+    }
   }
 }
 
@@ -165,8 +260,13 @@ cudaError_t launch_set_views(ViewDesc* dst, const ViewDesc* host, uint32_t n, cu
   return cudaGetLastError();
 }
 
+cudaError_t launch_count(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
+  tile_walk_kernel<false><<<grid_for(vs, s.num_sms), kWalkThreads, 0, st>>>(vs, b, 0);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st) {
-  emit_kernel<<<grid_for(vs, s.num_sms), 256, 0, st>>>(vs, b, deterministic);
+  tile_walk_kernel<true><<<grid_for(vs, s.num_sms), kWalkThreads, 0, st>>>(vs, b, deterministic);
   return cudaGetLastError();
 }
 

@@ -4,8 +4,9 @@
 // parameters are read once (the block stages its 256 x 40-byte transform
 // rows in shared memory with 128-bit loads), then for each view the thread
 // projects the Gaussian (project_forward.wgsl:19-96, project_visible.wgsl:
-// 233-310), counts the tiles it touches and the block compacts the visible
-// ones in global-id order with a decoupled look-back. This replaces the
+// 233-310) and the block compacts the visible ones in global-id order with a
+// decoupled look-back. The tiles each visible Gaussian touches are counted
+// afterwards by the warp-cooperative walk over the compact records. This replaces the
 // atomic compaction of project_forward.wgsl:94-96 (nondeterministic order)
 // and fuses the separate project_visible pass.
 //
@@ -78,11 +79,7 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
     const Cam<float> cam = cam_from_desc<float>(vd);
     Projected<float> p;
     p.visible = false;
-    uint32_t cnt = 0;
-    if (valid) {
-      p = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
-      if (p.visible) cnt = count_tiles(p, ts);
-    }
+    if (valid) p = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
     uint32_t tot;
     const uint32_t rank = block_exclusive_scan(p.visible ? 1u : 0u, s_scan, &tot);
     if (threadIdx.x == 0) {
@@ -103,7 +100,6 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
                          __uint_as_float(p.box.y0 | (p.box.y1 << 16)));
       slice(a.b.gid_of_c, a.b.Vcap, v)[c] = g;
       slice(a.b.depth_key, a.b.Vcap, v)[c] = __float_as_uint(p.depth);
-      slice(a.b.count, a.b.Vcap, v)[c] = cnt;
     }
   }
   epoch_end(a.ctl, epoch);
