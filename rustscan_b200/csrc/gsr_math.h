@@ -668,19 +668,34 @@ template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
 // 2^22; its integer then sits in the low mantissa bits) and the scaling by
 // 2^n done by adding n to the exponent field, exact because the result stays
 // a normal number for x >= -87.33. Same IEEE operations on host and device.
+// Constants of blend_expf (shared with the paired device version).
+namespace bexp {
+constexpr float kLog2e = 1.44269504088896341f;
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr uint32_t kMagicBits = 0x4B400000u;
+constexpr float kLn2Hi = 0.693145751953125f;
+constexpr float kLn2Lo = 1.42860682030941723e-06f;
+constexpr float kP7 = 1.98412698412698413e-04f;  // 1/7!
+constexpr float kP6 = 1.38888888888888889e-03f;  // 1/6!
+constexpr float kP5 = 8.33333333333333333e-03f;  // 1/5!
+constexpr float kP4 = 4.16666666666666667e-02f;  // 1/4!
+constexpr float kP3 = 1.66666666666666667e-01f;  // 1/3!
+constexpr float kLow = -87.3365f;                 // below: the result would not be normal
+}  // namespace bexp
+
 GSR_HD float blend_expf(float x) {
   x = fminf(x, 0.0f);
-  if (!(x > -87.3365f)) return (x != x) ? x : 0.0f;
-  const float t = eadd(emul(x, 1.44269504088896341f), 12582912.0f);
-  const float n = esub(t, 12582912.0f);
-  const int ni = (int)(float_to_bits(t) - 0x4B400000u);
-  float r = fmaf(-n, 0.693145751953125f, x);
-  r = fmaf(-n, 1.42860682030941723e-06f, r);
-  float p = 1.98412698412698413e-04f;
-  p = fmaf(p, r, 1.38888888888888889e-03f);
-  p = fmaf(p, r, 8.33333333333333333e-03f);
-  p = fmaf(p, r, 4.16666666666666667e-02f);
-  p = fmaf(p, r, 1.66666666666666667e-01f);
+  if (!(x > bexp::kLow)) return (x != x) ? x : 0.0f;
+  const float t = eadd(emul(x, bexp::kLog2e), bexp::kMagic);
+  const float n = esub(t, bexp::kMagic);
+  const int ni = (int)(float_to_bits(t) - bexp::kMagicBits);
+  float r = fmaf(-n, bexp::kLn2Hi, x);
+  r = fmaf(-n, bexp::kLn2Lo, r);
+  float p = bexp::kP7;
+  p = fmaf(p, r, bexp::kP6);
+  p = fmaf(p, r, bexp::kP5);
+  p = fmaf(p, r, bexp::kP4);
+  p = fmaf(p, r, bexp::kP3);
   p = fmaf(p, r, 0.5f);
   p = fmaf(p, r, 1.0f);
   p = fmaf(p, r, 1.0f);

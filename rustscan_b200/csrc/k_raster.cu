@@ -31,6 +31,12 @@ namespace gsr {
 
 namespace {
 
+// Pixels per lane. The forward gains nothing from more than 2; the
+// backward amortises its per-Gaussian warp reduction over twice the pixels
+// with 4 where the tile is tall enough for an 8 x 16 warp block (16x16).
+constexpr int kFwdPPL = 2;
+constexpr int kBwdPPL16 = 4;
+
 struct RasterArgs {
   ViewSet vs;
   FwdBufs b;
@@ -51,6 +57,7 @@ __device__ __forceinline__ uint32_t find_view(const ViewSet& vs, uint32_t item) 
 // Warp w of a TW-wide tile owns the 8 x (4*PPL) block at (x0, y0); lane l
 // owns column x0 + (l & 7) and rows y0 + (l >> 3) + 4q, q = 0..PPL-1.
 template <int TW, int PPL> struct WarpBlock {
+  static_assert(TW % 8 == 0, "tile width is a multiple of the 8-pixel warp block");
   static constexpr int kWarpsX = TW / 8;
   static constexpr int kRows = 4 * PPL;
   __device__ static int x0(int w) { return (w % kWarpsX) * 8; }
@@ -99,10 +106,62 @@ __device__ __forceinline__ int build_list(const uint8_t* s_mask, uint32_t nb, in
   return cnt;
 }
 
+// Paired FP32 arithmetic: every lane owns its pixels in pairs (rows y + 8k and
+// y + 8k + 4 of one column), and the per-pixel arithmetic of a pair runs as
+// two-wide operations (fma2 is a fused multiply-add per half, add2 and mul2
+// round per half like the scalar operations).
+//
+// The compiler may contract a paired multiply feeding a paired add into one
+// fused multiply-add (even when written with explicit rounding), which would
+// change the blend decisions. So every multiply-then-add whose result decides
+// a contributor (sigma, and the range reduction of the exponential) runs as
+// individually rounded scalar operations, and the paired operations are used
+// only where contraction cannot occur (a product feeding a comparison, a
+// multiply-add that is fused by definition, a sum feeding a product) or in
+// gradient arithmetic, which has no bit-exactness requirement.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// blend_sigma_shared for the two pixels of a pair (same column: same t1,
+// t2), individually rounded scalar operations.
+__device__ __forceinline__ float2 sigma2(float t1, float t2, float2 dy, float cc) {
+  return make_float2(blend_sigma_shared(t1, t2, dy.x, cc), blend_sigma_shared(t1, t2, dy.y, cc));
+}
+
+// blend_expf(-sigma) for both pixels. The argument is clamped to [-87, 0]
+// first, which leaves every sigma the contribution test can accept
+// (0 <= sigma <= log(255) + margin) unchanged, so for those the result is
+// bit-identical to blend_expf; for the others it stays finite.
+__device__ __forceinline__ float2 blend_exp2(float2 sigma) {
+  const float xx = fmaxf(fminf(-sigma.x, 0.f), -87.f), xy = fmaxf(fminf(-sigma.y, 0.f), -87.f);
+  const float2 x = make_float2(xx, xy);
+  const float2 t = make_float2(eadd(emul(xx, bexp::kLog2e), bexp::kMagic), eadd(emul(xy, bexp::kLog2e), bexp::kMagic));
+  const float2 n = add2(t, f2(-bexp::kMagic));
+  const uint32_t ex = (__float_as_uint(t.x) - bexp::kMagicBits) << 23;
+  const uint32_t ey = (__float_as_uint(t.y) - bexp::kMagicBits) << 23;
+  float2 r = fma2(neg2(n), f2(bexp::kLn2Hi), x);
+  r = fma2(neg2(n), f2(bexp::kLn2Lo), r);
+  float2 p = f2(bexp::kP7);
+  p = fma2(p, r, f2(bexp::kP6));
+  p = fma2(p, r, f2(bexp::kP5));
+  p = fma2(p, r, f2(bexp::kP4));
+  p = fma2(p, r, f2(bexp::kP3));
+  p = fma2(p, r, f2(0.5f));
+  p = fma2(p, r, f2(1.0f));
+  p = fma2(p, r, f2(1.0f));
+  return make_float2(__uint_as_float(__float_as_uint(p.x) + ex), __uint_as_float(__float_as_uint(p.y) + ey));
+}
+
 template <int TW, int TH, int PPL, int BATCH>
 __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) {
+  static_assert(PPL % 2 == 0, "pixels per lane come in pairs");
+  static_assert(TH % (4 * PPL) == 0 && (TW * TH / PPL) % 32 == 0, "warp blocks tile the tile");
   constexpr int NT = TW * TH / PPL;
   constexpr int NW = NT / 32;
+  constexpr int NP = PPL / 2;
   __shared__ float4 s_a[BATCH];  // x, y, conic a, 2 conic b
   __shared__ float4 s_b[BATCH];  // conic c, reject cut, opacity, -
   __shared__ float4 s_c[BATCH];  // max(r,0), max(g,0), max(b,0), -
@@ -125,16 +184,20 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
   uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
   const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
-  float T[PPL], C0[PPL], C1[PPL], C2[PPL], pcy[PPL];
+  // Pixel q = 2k + h sits at row pyb + 4q and is half h of pair k.
+  float2 T[NP], C0[NP], C1[NP], C2[NP], npcy[NP];
   uint32_t last[PPL], nc[PPL], stop[PPL];
   bool done[PPL];
   bool all_done = true;
 #pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    T[k] = f2(1.f);
+    C0[k] = C1[k] = C2[k] = f2(0.f);
+    npcy[k] = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
+  }
+#pragma unroll
   for (int q = 0; q < PPL; ++q) {
     const uint32_t py = pyb + 4 * q;
-    T[q] = 1.f;
-    C0[q] = C1[q] = C2[q] = 0.f;
-    pcy[q] = (float)py + 0.5f;
     last[q] = nc[q] = 0;
     stop[q] = s1;
     done[q] = !(px < vd.w && py < vd.h);
@@ -156,35 +219,52 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     __syncthreads();
     if (!__all_sync(0xffffffffu, all_done)) {
       const int cnt = build_list(s_mask, nb, warp, lane, s_list[warp]);
-      for (int k = 0; k < cnt; ++k) {
-        const uint32_t j = s_list[warp][k];
+      for (int e = 0; e < cnt; ++e) {
+        const uint32_t j = s_list[warp][e];
         const float4 A = s_a[j];
         const float4 B = s_b[j];
         const float dx = esub(A.x, pcx);
         const float t1 = emul(emul(A.z, dx), dx);
         const float t2 = emul(A.w, dx);
 #pragma unroll
-        for (int q = 0; q < PPL; ++q) {
-          if (done[q]) continue;
-          const float dy = esub(A.y, pcy[q]);
-          // blend_sigma's expression tree with a*dx*dx and 2b*dx shared.
-          const float sigma = blend_sigma_shared(t1, t2, dy, B.x);
-          if (sigma > B.y) continue;
-          float gauss;
-          const float alpha = blend_alpha_of(sigma, B.z, gauss);
-          if (alpha < 0.f) continue;
+        for (int k = 0; k < NP; ++k) {
+          const bool d0 = done[2 * k], d1 = done[2 * k + 1];
+          if (d0 && d1) continue;
+          const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
+          const float2 sg = sigma2(t1, t2, dy, B.x);
+          const bool l0 = !d0 && !(sg.x > B.y), l1 = !d1 && !(sg.y > B.y);
+          if (!(l0 || l1)) continue;
+          const float2 og = mul2(f2(B.z), blend_exp2(sg));
+          const float ax = fminf(0.999f, og.x), ay = fminf(0.999f, og.y);
+          // blend_alpha_of: sigma >= 0 and alpha >= 1/255.
+          const bool c0 = l0 && sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
+          const bool c1 = l1 && sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
+          if (!(c0 || c1)) continue;
+          // A pixel that does not take this Gaussian blends with alpha 0,
+          // which leaves its colour and transmittance bit for bit unchanged.
+          const float2 am = make_float2(c0 ? ax : 0.f, c1 ? ay : 0.f);
           const float4 Cc = s_c[j];
-          const float w = emul(alpha, T[q]);
-          C0[q] = fmaf(Cc.x, w, C0[q]);  // blend_accum; Cc was clamped at staging
-          C1[q] = fmaf(Cc.y, w, C1[q]);
-          C2[q] = fmaf(Cc.z, w, C2[q]);
-          T[q] = emul(T[q], esub(1.f, alpha));
-          last[q] = b0 + j + 1;
-          ++nc[q];
+          const float2 w = mul2(am, T[k]);
+          C0[k] = fma2(f2(Cc.x), w, C0[k]);  // blend_accum; Cc was clamped at staging
+          C1[k] = fma2(f2(Cc.y), w, C1[k]);
+          C2[k] = fma2(f2(Cc.z), w, C2[k]);
+          T[k] = mul2(T[k], add2(f2(1.f), neg2(am)));
           s_hit[j] = 1;
-          if (T[q] < 1e-4f) {
-            done[q] = true;
-            stop[q] = b0 + j + 1;
+          if (c0) {
+            last[2 * k] = b0 + j + 1;
+            ++nc[2 * k];
+            if (T[k].x < 1e-4f) {
+              done[2 * k] = true;
+              stop[2 * k] = b0 + j + 1;
+            }
+          }
+          if (c1) {
+            last[2 * k + 1] = b0 + j + 1;
+            ++nc[2 * k + 1];
+            if (T[k].y < 1e-4f) {
+              done[2 * k + 1] = true;
+              stop[2 * k + 1] = b0 + j + 1;
+            }
           }
         }
         all_done = true;
@@ -204,8 +284,13 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     const uint32_t py = pyb + 4 * q;
     if (!(px < vd.w && py < vd.h)) continue;
     const size_t pix = (size_t)py * vd.w + px;
-    out[pix] = make_float4(C0[q] + T[q] * a.bg[0], C1[q] + T[q] * a.bg[1], C2[q] + T[q] * a.bg[2], 1.f - T[q]);
-    slice(a.b.tfinal, a.b.Pcap, v)[pix] = T[q];
+    const int k = q / 2;
+    const float Tq = (q & 1) ? T[k].y : T[k].x;
+    const float c0 = (q & 1) ? C0[k].y : C0[k].x;
+    const float c1 = (q & 1) ? C1[k].y : C1[k].x;
+    const float c2 = (q & 1) ? C2[k].y : C2[k].x;
+    out[pix] = make_float4(c0 + Tq * a.bg[0], c1 + Tq * a.bg[1], c2 + Tq * a.bg[2], 1.f - Tq);
+    slice(a.b.tfinal, a.b.Pcap, v)[pix] = Tq;
     slice(a.b.last, a.b.Pcap, v)[pix] = last[q];
     slice(a.b.ncontrib, a.b.Pcap, v)[pix] = nc[q];
     slice(a.b.nvisit, a.b.Pcap, v)[pix] = stop[q] - s0;
@@ -246,73 +331,135 @@ __device__ __forceinline__ float warp_reduce_scatter16(float (&x)[16], int lane)
   return x[0] + __shfl_xor_sync(full, x[0], 1);
 }
 
-// Per-pixel state of the reverse walk.
-struct BwdPixel {
-  uint32_t last;
-  float T, K;
-  float vrgb[3];
-  float S[3];
+// Per-pair state of the reverse walk (pixel q = 2k + h is half h of pair k).
+struct BwdPair {
+  uint32_t last0, last1;
+  float2 T, K;          // transmittance, background term
+  float2 S0, S1, S2;    // colour accumulated behind the current Gaussian
+  float2 vr, vg, vb;
+  float2 npcy;
 };
 
-__device__ __forceinline__ void load_bwd_pixel(const RasterArgs& a, const ViewDesc& vd, uint32_t v, uint32_t px,
-                                               uint32_t py, BwdPixel& p) {
-  p.last = 0;
-  p.T = 1.f;
-  p.K = 0.f;
-  p.vrgb[0] = p.vrgb[1] = p.vrgb[2] = 0.f;
-  p.S[0] = p.S[1] = p.S[2] = 0.f;
-  if (!(px < vd.w && py < vd.h)) return;
-  const size_t pix = (size_t)py * vd.w + px;
-  p.last = slice(a.b.last, a.b.Pcap, v)[pix];
-  p.T = slice(a.b.tfinal, a.b.Pcap, v)[pix];
-  const float4 g = reinterpret_cast<const float4*>(a.v_rgba)[vd.pix_base + pix];
-  p.vrgb[0] = g.x;
-  p.vrgb[1] = g.y;
-  p.vrgb[2] = g.z;
-  p.K = (g.x * a.bg[0] + g.y * a.bg[1] + g.z * a.bg[2] - g.w) * p.T;
+__device__ __forceinline__ void load_bwd_pair(const RasterArgs& a, const ViewDesc& vd, uint32_t v, uint32_t px,
+                                              uint32_t py0, BwdPair& p) {
+  float T[2] = {1.f, 1.f}, K[2] = {0.f, 0.f}, g[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+  uint32_t last[2] = {0u, 0u};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t py = py0 + 4 * h;
+    if (!(px < vd.w && py < vd.h)) continue;
+    const size_t pix = (size_t)py * vd.w + px;
+    last[h] = slice(a.b.last, a.b.Pcap, v)[pix];
+    T[h] = slice(a.b.tfinal, a.b.Pcap, v)[pix];
+    const float4 u = reinterpret_cast<const float4*>(a.v_rgba)[vd.pix_base + pix];
+    g[h][0] = u.x;
+    g[h][1] = u.y;
+    g[h][2] = u.z;
+    K[h] = (u.x * a.bg[0] + u.y * a.bg[1] + u.z * a.bg[2] - u.w) * T[h];
+  }
+  p.last0 = last[0];
+  p.last1 = last[1];
+  p.T = make_float2(T[0], T[1]);
+  p.K = make_float2(K[0], K[1]);
+  p.S0 = p.S1 = p.S2 = f2(0.f);
+  p.vr = make_float2(g[0][0], g[1][0]);
+  p.vg = make_float2(g[0][1], g[1][1]);
+  p.vb = make_float2(g[0][2], g[1][2]);
+  p.npcy = make_float2(-((float)py0 + 0.5f), -((float)(py0 + 4) + 0.5f));
 }
 
-// One pixel's step of the reverse walk; adds its gradient into x[0..11)
-// (the contributor count is taken from a ballot).
-__device__ __forceinline__ bool bwd_step(BwdPixel& p, uint32_t s, float dx, float t1, float t2, float pcy,
-                                         const float4& A, const float4& B, const float4& Cc, int ref_mode,
-                                         float (&x)[16]) {
-  if (s >= p.last) return false;
-  const float dy = esub(A.y, pcy);
-  const float sigma = blend_sigma_shared(t1, t2, dy, B.x);
-  if (sigma > B.y) return false;
-  float gauss;
-  const float alpha = blend_alpha_of(sigma, B.z, gauss);
-  if (alpha < 0.f) return false;
-  const bool skip = ref_mode && (p.T <= 1e-4f);
-  SplatGrad<float> g;
-  blend_step_grad(dx, dy, A.z, 0.5f * A.w, B.x, Cc.x, Cc.y, Cc.z, B.z, gauss, alpha, p.T, p.S, p.vrgb, p.K, skip, g);
-  if (skip) return false;
-  x[0] += g.v_xy[0];
-  x[1] += g.v_xy[1];
-  x[2] += g.v_conic[0];
-  x[3] += g.v_conic[1];
-  x[4] += g.v_conic[2];
-  x[5] += g.v_rgb[0];
-  x[6] += g.v_rgb[1];
-  x[7] += g.v_rgb[2];
-  x[8] += g.v_opac;
-  x[9] += g.abs_xy[0];
-  x[10] += g.abs_xy[1];
-  return true;
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// One step of the reverse walk for both pixels of a pair: the contribution
+// decisions repeat the forward's bit for bit; the gradient follows
+// blend_step_grad (rasterize_backwards, exact adjoint), with the
+// transmittance recovered with a Newton-refined hardware reciprocal. Adds the pair's gradient into x[0..11) and returns, per
+// pixel, whether it counts as a contributor (in the reference semantics a
+// pixel whose transmittance fell to 1e-4 no longer does).
+__device__ __forceinline__ uint32_t bwd_pair_step(BwdPair& p, uint32_t s, float dx, float t1, float t2, float hdx2,
+                                                  const float4& A, const float4& B, const float4& Cc, int ref_mode,
+                                                  float (&x)[16]) {
+  const bool in0 = s < p.last0, in1 = s < p.last1;
+  if (!(in0 || in1)) return 0u;
+  const float2 dy = make_float2(eadd(A.y, p.npcy.x), eadd(A.y, p.npcy.y));
+  const float2 sg = sigma2(t1, t2, dy, B.x);
+  const bool l0 = in0 && !(sg.x > B.y), l1 = in1 && !(sg.y > B.y);
+  if (!(l0 || l1)) return 0u;
+  const float2 gs = blend_exp2(sg);
+  const float2 og = mul2(f2(B.z), gs);
+  const float ax = fminf(0.999f, og.x), ay = fminf(0.999f, og.y);
+  const bool c0 = l0 && sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
+  const bool c1 = l1 && sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
+  if (!(c0 || c1)) return 0u;
+  const bool sk0 = ref_mode && p.T.x <= 1e-4f, sk1 = ref_mode && p.T.y <= 1e-4f;
+  const float2 al = make_float2(ax, ay);
+  const float2 am = make_float2(c0 ? ax : 0.f, c1 ? ay : 0.f);
+  const float2 om = add2(f2(1.f), neg2(am));
+  // Hardware reciprocal refined by one Newton step (r + r(1 - om r)); a
+  // pixel that does not take this Gaussian keeps its transmittance exactly.
+#ifdef GSR_EXACT_RCP
+  float2 ra = make_float2(__frcp_rn(om.x), __frcp_rn(om.y));
+#else
+  float2 ra = make_float2(rcp_approx(om.x), rcp_approx(om.y));
+  ra = fma2(ra, fma2(neg2(om), ra, f2(1.f)), ra);
+#endif
+  ra = make_float2(c0 ? ra.x : 1.f, c1 ? ra.y : 1.f);
+  const float2 Ti = mul2(p.T, ra);
+  const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
+  const float2 cpv = fma2(f2(cp2), p.vb, fma2(f2(cp1), p.vg, mul2(f2(cp0), p.vr)));
+  const float2 vis = mul2(am, Ti);
+  const float2 sv = fma2(p.S2, p.vb, fma2(p.S1, p.vg, mul2(p.S0, p.vr)));
+  const float2 va = fma2(Ti, cpv, neg2(mul2(add2(sv, p.K), ra)));
+  p.S0 = fma2(f2(cp0), vis, p.S0);
+  p.S1 = fma2(f2(cp1), vis, p.S1);
+  p.S2 = fma2(f2(cp2), vis, p.S2);
+  p.T = Ti;
+  const bool gm0 = c0 && !sk0, gm1 = c1 && !sk1;
+  const bool gg0 = gm0 && og.x <= 0.999f, gg1 = gm1 && og.y <= 0.999f;
+  const float2 visg = make_float2(gm0 ? vis.x : 0.f, gm1 ? vis.y : 0.f);
+  const float2 av = mul2(al, va);
+  const float2 vs = make_float2(gg0 ? -av.x : 0.f, gg1 ? -av.y : 0.f);
+  const float2 vo = mul2(va, gs);
+  const float2 vsdy = mul2(vs, dy);
+  const float ca = A.z, cb = 0.5f * A.w, cc = B.x;
+  const float2 vxy0 = mul2(vs, fma2(f2(cb), dy, f2(ca * dx)));
+  const float2 vxy1 = mul2(vs, fma2(f2(cc), dy, f2(cb * dx)));
+  const float2 vc0 = mul2(vs, f2(hdx2));
+  const float2 vc1 = mul2(vsdy, f2(dx));
+  const float2 vc2 = mul2(vsdy, mul2(f2(0.5f), dy));
+  const float2 vr = mul2(visg, p.vr), vg = mul2(visg, p.vg), vb = mul2(visg, p.vb);
+  x[0] += vxy0.x + vxy0.y;
+  x[1] += vxy1.x + vxy1.y;
+  x[2] += vc0.x + vc0.y;
+  x[3] += vc1.x + vc1.y;
+  x[4] += vc2.x + vc2.y;
+  x[5] += vr.x + vr.y;
+  x[6] += vg.x + vg.y;
+  x[7] += vb.x + vb.y;
+  x[8] += (gg0 ? vo.x : 0.f) + (gg1 ? vo.y : 0.f);
+  x[9] += fabsf(vxy0.x) + fabsf(vxy0.y);
+  x[10] += fabsf(vxy1.x) + fabsf(vxy1.y);
+  return (gm0 ? 1u : 0u) | (gm1 ? 2u : 0u);
 }
 
 template <int TW, int TH, int PPL, int BATCH>
 __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) {
+  static_assert(PPL % 2 == 0, "pixels per lane come in pairs");
+  static_assert(TH % (4 * PPL) == 0 && (TW * TH / PPL) % 32 == 0, "warp blocks tile the tile");
   constexpr int NT = TW * TH / PPL;
   constexpr int NW = NT / 32;
+  constexpr int NP = PPL / 2;
   __shared__ float4 s_a[BATCH];
   __shared__ float4 s_b[BATCH];
   __shared__ float4 s_c[BATCH];
   __shared__ uint32_t s_cidx[BATCH];
   __shared__ uint8_t s_mask[BATCH];
   __shared__ uint16_t s_list[NW][BATCH];
-  __shared__ float s_part[NW][BATCH][12];
+  __shared__ float4 s_part[NW][BATCH][3];
   __shared__ uint32_t s_max;
   const uint32_t item = blockIdx.x;
   const uint32_t v = find_view(a.vs, item);
@@ -330,12 +477,12 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
   float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
   const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
-  BwdPixel pp[PPL];
+  BwdPair pp[NP];
   uint32_t mylast = 0;
 #pragma unroll
-  for (int q = 0; q < PPL; ++q) {
-    load_bwd_pixel(a, vd, v, px, pyb + 4 * q, pp[q]);
-    mylast = max(mylast, pp[q].last);
+  for (int k = 0; k < NP; ++k) {
+    load_bwd_pair(a, vd, v, px, pyb + 8 * k, pp[k]);
+    mylast = max(mylast, max(pp[k].last0, pp[k].last1));
   }
   if (threadIdx.x == 0) s_max = 0;
   __syncthreads();
@@ -356,15 +503,15 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
       s_c[j] = Cc;
       s_cidx[j] = c;
     }
-    for (uint32_t q = threadIdx.x; q < (uint32_t)NW * nb * 12; q += NT) {
-      const uint32_t w = q / (nb * 12), r = q % (nb * 12);
-      s_part[w][r / 12][r % 12] = 0.f;
+    {
+      float4* z = &s_part[0][0][0];
+      for (uint32_t q = threadIdx.x; q < (uint32_t)(NW * BATCH * 3); q += NT) z[q] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
     if (bs < wmax) {
       const int cnt = build_list(s_mask, nb, warp, lane, s_list[warp]);
-      for (int k = cnt - 1; k >= 0; --k) {
-        const uint32_t j = s_list[warp][k];
+      for (int e = cnt - 1; e >= 0; --e) {
+        const uint32_t j = s_list[warp][e];
         const uint32_t s = bs + j;
         if (s >= wmax) continue;  // warp-uniform
         const float4 A = s_a[j];
@@ -373,33 +520,38 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
         const float dx = esub(A.x, pcx);
         const float t1 = emul(emul(A.z, dx), dx);
         const float t2 = emul(A.w, dx);
+        const float hdx2 = 0.5f * dx * dx;
         float x[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) x[i] = 0.f;
         uint32_t ncontrib = 0;
 #pragma unroll
-        for (int q = 0; q < PPL; ++q) {
-          const bool c = bwd_step(pp[q], s, dx, t1, t2, (float)(pyb + 4 * q) + 0.5f, A, B, Cc, a.ref_mode, x);
-          ncontrib += __popc(__ballot_sync(0xffffffffu, c));
+        for (int k = 0; k < NP; ++k) {
+          const uint32_t cb = bwd_pair_step(pp[k], s, dx, t1, t2, hdx2, A, B, Cc, a.ref_mode, x);
+          ncontrib += __popc(__ballot_sync(0xffffffffu, cb & 1u)) + __popc(__ballot_sync(0xffffffffu, cb & 2u));
         }
         if (ncontrib) {
-          const float r = warp_reduce_scatter16(x, lane);
+          float r = warp_reduce_scatter16(x, lane);
           const int slot = lane >> 1;
-          if ((lane & 1) == 0 && slot < 11) s_part[warp][j][slot] = r;
-          if (lane == 0) s_part[warp][j][11] = (float)ncontrib;
+          // v_rgb is zero for a channel whose raw colour is negative.
+          if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
+          float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
+          if ((lane & 1) == 0 && slot < 11) sp[slot] = r;
+          if (lane == 0) sp[11] = (float)ncontrib;
         }
       }
     }
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < nb * 3; q += NT) {
       const uint32_t j = q / 3, k = q % 3;
-      float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 f = s_part[0][j][k];
 #pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        f.x = f.x + s_part[w][j][4 * k + 0];
-        f.y = f.y + s_part[w][j][4 * k + 1];
-        f.z = f.z + s_part[w][j][4 * k + 2];
-        f.w = f.w + s_part[w][j][4 * k + 3];
+      for (int w = 1; w < NW; ++w) {
+        const float4 g = s_part[w][j][k];
+        f.x = f.x + g.x;
+        f.y = f.y + g.y;
+        f.z = f.z + g.z;
+        f.w = f.w + g.w;
       }
       if (a.det) {
         reinterpret_cast<float4*>(part + (size_t)(bs + j) * 12)[k] = f;
@@ -446,9 +598,9 @@ cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, fl
   cudaError_t e = cudaMemsetAsync(b.visible_c, 0, b.Vcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, 2>(a, vs.total_tiles, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, 2>(a, vs.total_tiles, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, 2>(a, vs.total_tiles, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, kFwdPPL>(a, vs.total_tiles, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, kFwdPPL>(a, vs.total_tiles, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, kFwdPPL>(a, vs.total_tiles, st);
   return cudaErrorInvalidValue;
 }
 
@@ -469,7 +621,7 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     if (e != cudaSuccess) return e;
   }
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, 2>(a, vs.total_tiles, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.total_tiles, st);
   if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.total_tiles, st);
   if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.total_tiles, st);
   return cudaErrorInvalidValue;
