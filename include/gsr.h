@@ -60,7 +60,8 @@ typedef struct gsr_config {
   float cov_blur;          /* screen-space covariance blur in px^2 (0.3) */
   float background[3];     /* background colour (0,0,0) */
   uint32_t tile_w, tile_h; /* tile shape: 16x16 (default), 8x8 or 32x8 */
-  uint32_t batch;          /* Gaussians staged in shared memory per batch (0: 256) */
+  uint32_t batch;          /* Gaussians staged in shared memory per raster batch: 64, 128 or 256
+                              (rounded up; 0: tuned defaults, 128 forward / 64 backward) */
   int32_t sh_dtype;        /* GSR_SH_F32 or GSR_SH_BF16 storage of SH coefficients */
   int32_t adjoint;         /* GSR_ADJOINT_EXACT (default) or GSR_ADJOINT_REFERENCE */
   int32_t deterministic;   /* 1: fixed-order gradient reduction, bitwise reruns */
@@ -252,6 +253,32 @@ GSR_API gsr_status gsr_train_step(gsr_ctx* ctx, float* transforms, void* sh, flo
                           uint32_t sh_degree, const gsr_adam_state* state, const gsr_camera* cams, uint32_t n_views,
                           const float* targets, const gsr_train_params* params, float* densify_acc, float* loss,
                           int32_t use_graph, void* stream);
+
+/* ---- autotuner (no counterpart in the reference) ------------------------ */
+/* Candidates: tile shapes 16x16, 8x8, 32x8 times raster batches 64, 128,
+ * 256 (9 entries, in that order). */
+enum { GSR_TUNE_CANDIDATES = 9 };
+typedef struct gsr_tune_candidate {
+  uint32_t tile_w, tile_h, batch;
+  int32_t status;   /* GSR_OK, or why the candidate could not run */
+  float ms_per_view; /* forward + backward, mean over the timed repetitions */
+  uint32_t _pad;
+} gsr_tune_candidate;
+typedef struct gsr_tune_result {
+  uint32_t tile_w, tile_h, batch; /* the fastest candidate */
+  float ms_per_view;
+  gsr_tune_candidate candidates[GSR_TUNE_CANDIDATES];
+} gsr_tune_result;
+
+/* Times forward + backward (a fixed upstream gradient) of the given splats
+ * and views for every candidate, each in a temporary context built from
+ * *base with that tile shape and batch (and max_isects grown as needed), and
+ * reports the fastest; base->tile_w/tile_h/batch are ignored. reps >= 1 timed
+ * repetitions after one warm-up. Allocates and frees device memory and
+ * synchronises the stream: call it once per scene/resolution mix, outside
+ * any stream capture, then create the working context with the result. */
+GSR_API gsr_status gsr_autotune(const gsr_config* base, const gsr_splats* splats, const gsr_camera* cams,
+                                uint32_t n_views, int32_t reps, gsr_tune_result* out, void* stream);
 
 /* ---- instrumentation (no counterpart in the reference) ------------------ */
 /* Stage timing: when enabled, the context records CUDA events on the stream

@@ -74,6 +74,7 @@ template <class F> struct FwdState {
   orc_camera camera;
   Cam<F> cam;
   F cov_blur;
+  bool hp = false;  // FP64 2D-covariance compensation and inversion
   F bg[3];
   TileShape ts;
   uint32_t tiles_x = 0, tiles_y = 0;
@@ -119,7 +120,7 @@ template <class F> void forward(FwdState<F>& st) {
     V3<F> mean{t[0], t[1], t[2]};
     V4<F> q{t[3], t[4], t[5], t[6]};
     V3<F> ls{t[7], t[8], t[9]};
-    all[g] = project_gaussian(cam, mean, q, ls, sp.raw_opac[g], st.cov_blur, st.ts, st.tiles_x, st.tiles_y);
+    all[g] = project_gaussian(cam, mean, q, ls, sp.raw_opac[g], st.cov_blur, st.ts, st.tiles_x, st.tiles_y, st.hp);
     if (all[g].visible) cnt[g] = count_tiles(all[g], st.ts);
   }
   // Compaction in global-id order (replaces the atomic compaction of
@@ -399,7 +400,7 @@ void project_backward_all(const FwdState<F>& st, const BwdOut<F>& bo, bool exact
     V3<F> vcon{sg.v_conic[0], sg.v_conic[1], sg.v_conic[2]};
     V3<F> vcol{sg.v_rgb[0], sg.v_rgb[1], sg.v_rgb[2]};
     const ParamGrad<F> pg = project_backward(st.cam, mean, q, ls, sp.raw_opac[g], st.cov_blur, vxy, vcon, vcol,
-                                             sg.v_opac, sp.degree, coeff, exact);
+                                             sg.v_opac, sp.degree, coeff, exact, true, st.hp);
     // helpers.wgsl:289-380: SH coefficient gradients.
     F b[25];
     sh_basis<F>(sp.degree, pg.viewdir.x, pg.viewdir.y, pg.viewdir.z, b);
@@ -591,7 +592,7 @@ ORC_EXPORT float orc_logf(float x) { return portable_logf(x); }
 #define ORC_FWD_IMPL(SUF, F)                                                                                    \
   ORC_EXPORT orc_fwd_##SUF* orc_forward_##SUF(const F* transforms, const F* sh, const F* raw_opac, int n,         \
                                               int degree, const orc_camera* cam, F cov_blur, const F* bg,         \
-                                              uint32_t tile_w, uint32_t tile_h) {                                 \
+                                              uint32_t tile_w, uint32_t tile_h, int hp) {                         \
     orc_fwd_##SUF* h = new orc_fwd_##SUF();                                                                       \
     FwdState<F>& st = h->st;                                                                                      \
     st.sp.n = n;                                                                                                  \
@@ -603,6 +604,7 @@ ORC_EXPORT float orc_logf(float x) { return portable_logf(x); }
     st.camera = *cam;                                                                                             \
     st.cam = make_cam<F>(*cam);                                                                                   \
     st.cov_blur = cov_blur;                                                                                       \
+    st.hp = hp != 0;                                                                                              \
     st.bg[0] = bg[0];                                                                                             \
     st.bg[1] = bg[1];                                                                                             \
     st.bg[2] = bg[2];                                                                                             \

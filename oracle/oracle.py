@@ -42,7 +42,7 @@ def lib():
         L.orc_logf.restype = C.c_float
         for suf, fp, ft in (("f32", f32p, C.c_float), ("f64", f64p, C.c_double)):
             f = getattr(L, f"orc_forward_{suf}")
-            f.argtypes = [fp, fp, fp, C.c_int, C.c_int, C.c_void_p, ft, fp, C.c_uint32, C.c_uint32]
+            f.argtypes = [fp, fp, fp, C.c_int, C.c_int, C.c_void_p, ft, fp, C.c_uint32, C.c_uint32, C.c_int]
             f.restype = C.c_void_p
             getattr(L, f"orc_free_{suf}").argtypes = [C.c_void_p]
             getattr(L, f"orc_sizes_{suf}").argtypes = [C.c_void_p, u64p]
@@ -92,7 +92,7 @@ class Forward:
     """Oracle forward pass of one view; keeps the inputs alive for the backward."""
 
     def __init__(self, transforms, sh, raw_opacity, degree, camera, cov_blur=0.3, background=(0.0, 0.0, 0.0),
-                 tile=(16, 16), f64=False):
+                 tile=(16, 16), f64=False, fp64_conic=False):
         self.f64 = f64
         dt = np.float64 if f64 else np.float32
         fp = f64p if f64 else f32p
@@ -112,7 +112,7 @@ class Forward:
         self._h = getattr(L, f"orc_forward_{self.suf}")(
             _p(self.transforms, fp), _p(self.sh, fp), _p(self.raw_opacity, fp), self.n, self.degree,
             self._cam_rec.ctypes.data, (C.c_double if f64 else C.c_float)(cov_blur), _p(self.bg, fp),
-            tile[0], tile[1])
+            tile[0], tile[1], int(bool(fp64_conic)))
         sizes = np.zeros(4, dtype=np.uint64)
         getattr(L, f"orc_sizes_{self.suf}")(self._h, _p(sizes, u64p))
         self.num_visible, self.num_intersections, self.tiles_x, self.tiles_y = (int(v) for v in sizes)

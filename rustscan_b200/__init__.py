@@ -97,6 +97,49 @@ def host_splats_to_device(scene, device="cuda", sh_dtype=torch.float32) -> Devic
     )
 
 
+def make_config(max_splats, max_views=1, max_pixels=1920 * 1080, max_isects=0, tile=(16, 16), sh_dtype="f32",
+                adjoint="exact", deterministic=False, fp64_conic=False, cov_blur=DEFAULT_RASTER_COV_BLUR,
+                background=(0.0, 0.0, 0.0), batch=0) -> _lib.gsr_config:
+    """The gsr_config of a context (include/gsr.h)."""
+    cfg = _lib.gsr_config()
+    cfg.cov_blur = float(cov_blur)
+    for i in range(3):
+        cfg.background[i] = float(background[i])
+    cfg.tile_w, cfg.tile_h = int(tile[0]), int(tile[1])
+    cfg.batch = int(batch)
+    cfg.sh_dtype = _lib.GSR_SH_BF16 if sh_dtype in ("bf16", torch.bfloat16) else _lib.GSR_SH_F32
+    cfg.adjoint = _lib.GSR_ADJOINT_REFERENCE if adjoint == "reference" else _lib.GSR_ADJOINT_EXACT
+    cfg.deterministic = int(bool(deterministic))
+    cfg.fp64_conic = int(bool(fp64_conic))
+    cfg.max_splats = int(max_splats)
+    cfg.max_views = int(max_views)
+    cfg.max_pixels = int(max_pixels)
+    cfg.max_isects = int(max_isects)
+    return cfg
+
+
+def autotune(splats: "DeviceSplats", cameras, reps=3, **config) -> dict:
+    """Pick the tile shape and raster batch for this scene and view mix
+    (gsr_autotune): times forward + backward of every candidate in a
+    temporary context and returns the fastest plus the full table. The
+    keyword arguments are those of Context (tile and batch are ignored)."""
+    _require_cuda()
+    lib = _lib.load()
+    config.setdefault("max_splats", splats.num_splats())
+    config.setdefault("max_views", len(cameras))
+    config.setdefault("max_pixels", max(c.width * c.height for c in cameras))
+    cfg = make_config(**config)
+    res = _lib.gsr_tune_result()
+    sp = splats.struct()
+    cams = camera_array(cameras)
+    st = lib.gsr_autotune(C.byref(cfg), C.byref(sp), cams, len(cameras), int(reps), C.byref(res), _stream())
+    if st != _lib.GSR_OK:
+        raise GsrError(st, "gsr_autotune found no candidate that runs")
+    table = [dict(tile=(c.tile_w, c.tile_h), batch=c.batch, status=c.status, ms_per_view=c.ms_per_view)
+             for c in res.candidates]
+    return dict(tile=(res.tile_w, res.tile_h), batch=res.batch, ms_per_view=res.ms_per_view, candidates=table)
+
+
 class Context:
     """Owns the library context (scratch, saved forward state) for one stream."""
 
@@ -105,20 +148,8 @@ class Context:
                  cov_blur=DEFAULT_RASTER_COV_BLUR, background=(0.0, 0.0, 0.0), batch=0):
         _require_cuda()
         self._lib = _lib.load()
-        cfg = _lib.gsr_config()
-        cfg.cov_blur = float(cov_blur)
-        for i in range(3):
-            cfg.background[i] = float(background[i])
-        cfg.tile_w, cfg.tile_h = int(tile[0]), int(tile[1])
-        cfg.batch = int(batch)
-        cfg.sh_dtype = _lib.GSR_SH_BF16 if sh_dtype in ("bf16", torch.bfloat16) else _lib.GSR_SH_F32
-        cfg.adjoint = _lib.GSR_ADJOINT_REFERENCE if adjoint == "reference" else _lib.GSR_ADJOINT_EXACT
-        cfg.deterministic = int(bool(deterministic))
-        cfg.fp64_conic = int(bool(fp64_conic))
-        cfg.max_splats = int(max_splats)
-        cfg.max_views = int(max_views)
-        cfg.max_pixels = int(max_pixels)
-        cfg.max_isects = int(max_isects)
+        cfg = make_config(max_splats, max_views, max_pixels, max_isects, tile, sh_dtype, adjoint, deterministic,
+                          fp64_conic, cov_blur, background, batch)
         self.cfg = cfg
         self.background = tuple(float(b) for b in background)
         h = C.c_void_p()

@@ -110,6 +110,19 @@ class gsr_train_params(C.Structure):
     ]
 
 
+GSR_TUNE_CANDIDATES = 9
+
+
+class gsr_tune_candidate(C.Structure):
+    _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("batch", C.c_uint32), ("status", C.c_int32),
+                ("ms_per_view", C.c_float), ("_pad", C.c_uint32)]
+
+
+class gsr_tune_result(C.Structure):
+    _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("batch", C.c_uint32), ("ms_per_view", C.c_float),
+                ("candidates", gsr_tune_candidate * GSR_TUNE_CANDIDATES)]
+
+
 EXPORTED = [
     "gsr_create",
     "gsr_destroy",
@@ -130,6 +143,7 @@ EXPORTED = [
     "gsr_profile",
     "gsr_profile_read",
     "gsr_graph_kernel_count",
+    "gsr_autotune",
 ]
 
 PROFILE_STAGES = ("project", "depth_sort", "offsets", "emit", "tile_sort", "ranges", "raster_fwd", "visible", "loss",
@@ -176,6 +190,8 @@ def load():
     L.gsr_profile.argtypes = [vp, i32]
     L.gsr_profile_read.argtypes = [vp, C.POINTER(C.c_float), i32, vp]
     L.gsr_graph_kernel_count.argtypes = [vp]
+    L.gsr_autotune.argtypes = [C.POINTER(gsr_config), C.POINTER(gsr_splats), C.POINTER(gsr_camera), u32, i32,
+                               C.POINTER(gsr_tune_result), vp]
     for name in EXPORTED:
         if name not in ("gsr_destroy", "gsr_last_error", "gsr_version"):
             getattr(L, name).restype = C.c_int

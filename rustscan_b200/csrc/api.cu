@@ -234,6 +234,7 @@ gsr_status build_views(gsr_ctx* c, const gsr_camera* cams, uint32_t n_views, std
   vs.n_views = n_views;
   vs.tile_w = c->cfg.tile_w;
   vs.tile_h = c->cfg.tile_h;
+  vs.batch = c->cfg.batch;
   vs.total_tiles = tile_base;
   vs.max_tiles = max_tiles;
   return GSR_OK;
@@ -338,7 +339,6 @@ gsr_status gsr_create(const gsr_config* cfg_in, gsr_ctx** out) {
     cfg.tile_w = 16;
     cfg.tile_h = 16;
   }
-  if (cfg.batch == 0) cfg.batch = 256;
   if (cfg.max_views == 0) cfg.max_views = 1;
   if (cfg.max_splats == 0) cfg.max_splats = 1u << 16;
   if (cfg.max_pixels == 0) cfg.max_pixels = 1920ull * 1080ull;
@@ -468,6 +468,7 @@ gsr_status gsr_render_backward(gsr_ctx* c, const gsr_splats* sp, const float* v_
   pa.densify_acc = nullptr;
   pa.grad_scale = 1.0f;
   pa.exact = c->cfg.adjoint == GSR_ADJOINT_EXACT;
+  pa.hp = c->cfg.fp64_conic;
   prof_mark(c, kStProjectBwd, st);
   GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, st, c->num_sms));
   prof_mark(c, kStCount, st);
@@ -611,6 +612,7 @@ static gsr_status train_body(gsr_ctx* c, const gsr_splats* sp, float* transforms
   pa.use_visible = p->use_visible;
   pa.grad_scale = 1.0f / (float)n_views;
   pa.exact = c->cfg.adjoint == GSR_ADJOINT_EXACT;
+  pa.hp = c->cfg.fp64_conic;
   prof_mark(c, kStProjectBwd, st);
   GSR_CUDA(c, launch_project_bwd(splats_dev(c, sp), c->fwd_vs, c->cfg.cov_blur, c->b, pa, st, c->num_sms));
   prof_mark(c, kStAdam, st);
@@ -714,5 +716,94 @@ gsr_status gsr_profile_read(gsr_ctx* c, float* ms_per_stage, int32_t n_stages, v
 }
 
 int32_t gsr_graph_kernel_count(const gsr_ctx* c) { return c ? c->graph_kernels : 0; }
+
+gsr_status gsr_autotune(const gsr_config* base, const gsr_splats* sp, const gsr_camera* cams, uint32_t n_views,
+                        int32_t reps, gsr_tune_result* out, void* stream) {
+  if (!base || !sp || !cams || !out || n_views == 0 || reps < 1 || sp->sh_degree > 4) return GSR_ERR_INVALID_ARG;
+  memset(out, 0, sizeof(*out));
+  cudaStream_t st = (cudaStream_t)stream;
+  uint64_t pix = 0;
+  for (uint32_t v = 0; v < n_views; ++v) pix += (uint64_t)cams[v].width * cams[v].height;
+  const uint64_t n = sp->n, K = (uint64_t)(sp->sh_degree + 1) * (sp->sh_degree + 1);
+  float *rgba = nullptr, *vrgba = nullptr, *grads = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto release = [&]() {
+    if (rgba) cudaFree(rgba);
+    if (vrgba) cudaFree(vrgba);
+    if (grads) cudaFree(grads);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  if (cudaMalloc(&rgba, sizeof(float) * 4 * std::max<uint64_t>(pix, 1)) != cudaSuccess ||
+      cudaMalloc(&vrgba, sizeof(float) * 4 * std::max<uint64_t>(pix, 1)) != cudaSuccess ||
+      cudaMalloc(&grads, sizeof(float) * std::max<uint64_t>(n * (11 + 3 * K), 1)) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    release();
+    return GSR_ERR_OOM;
+  }
+  // A fixed upstream gradient (every float 0x3f3f3f3f, about 0.75): the work
+  // of the backward does not depend on its values.
+  if (cudaMemsetAsync(vrgba, 0x3f, sizeof(float) * 4 * pix, st) != cudaSuccess) {
+    release();
+    return GSR_ERR_CUDA;
+  }
+  const gsr_grads g{grads, grads + n * 10, grads + n * (10 + 3 * K)};
+  static const uint32_t kShapes[3][2] = {{16, 16}, {8, 8}, {32, 8}};
+  static const uint32_t kBatches[3] = {64, 128, 256};
+  float best = -1.f;
+  gsr_status first_err = GSR_OK;
+  for (int si = 0; si < 3; ++si) {
+    for (int bi = 0; bi < 3; ++bi) {
+      gsr_tune_candidate& cd = out->candidates[si * 3 + bi];
+      cd.tile_w = kShapes[si][0];
+      cd.tile_h = kShapes[si][1];
+      cd.batch = kBatches[bi];
+      cd.ms_per_view = -1.f;
+      gsr_config cfg = *base;
+      cfg.tile_w = cd.tile_w;
+      cfg.tile_h = cd.tile_h;
+      cfg.batch = cd.batch;
+      if (cfg.max_views < n_views) cfg.max_views = n_views;
+      gsr_ctx* c = nullptr;
+      gsr_status rs = gsr_create(&cfg, &c);
+      auto once = [&]() -> gsr_status {
+        gsr_status r = gsr_render_forward(c, sp, cams, n_views, rgba, nullptr, stream);
+        return r != GSR_OK ? r : gsr_render_backward(c, sp, vrgba, &g, nullptr, stream);
+      };
+      uint64_t req = 0;
+      if (rs == GSR_OK) rs = once();
+      if (rs == GSR_OK) rs = gsr_sync_status(c, stream, &req);
+      if (rs == GSR_ERR_CAPACITY) {
+        // Smaller tiles duplicate more keys: grow the capacity once.
+        rs = gsr_reserve_isects(c, std::min<uint64_t>(req + req / 8 + 4096, (1ull << 30) - 1));
+        if (rs == GSR_OK) rs = once();
+        if (rs == GSR_OK) rs = gsr_sync_status(c, stream, &req);
+      }
+      if (rs == GSR_OK) {
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps && rs == GSR_OK; ++r) rs = once();
+        cudaEventRecord(e1, st);
+        if (rs == GSR_OK) rs = gsr_sync_status(c, stream, &req);
+        float ms = 0.f;
+        if (rs == GSR_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+          cd.ms_per_view = ms / (float)reps / (float)n_views;
+          if (best < 0.f || cd.ms_per_view < best) {
+            best = cd.ms_per_view;
+            out->tile_w = cd.tile_w;
+            out->tile_h = cd.tile_h;
+            out->batch = cd.batch;
+            out->ms_per_view = best;
+          }
+        }
+      }
+      cd.status = rs;
+      if (rs != GSR_OK && first_err == GSR_OK) first_err = rs;
+      if (c) gsr_destroy(c);
+    }
+  }
+  release();
+  if (best < 0.f) return first_err != GSR_OK ? first_err : GSR_ERR_CUDA;
+  return GSR_OK;
+}
 
 }  // extern "C"

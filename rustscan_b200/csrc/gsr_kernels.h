@@ -45,6 +45,7 @@ struct ViewSet {
   const ViewDesc* views;  // device
   uint32_t n_views;
   uint32_t tile_w, tile_h;
+  uint32_t batch;         // Gaussians per shared-memory batch of the rasterizer (0: tuned defaults)
   uint32_t total_tiles;   // sum over views of tiles_x * tiles_y
   uint32_t max_tiles;     // max over views
 };
@@ -157,6 +158,7 @@ struct ProjBwdArgs {
   int use_visible;
   float grad_scale;
   int exact;
+  int hp;  // FP64 conic mode of the forward
 };
 cudaError_t launch_project_bwd(const SplatsDev& sp, const ViewSet& vs, float cov_blur, FwdBufs& b,
                                const ProjBwdArgs& a, cudaStream_t st, int num_sms);

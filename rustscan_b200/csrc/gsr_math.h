@@ -978,12 +978,14 @@ GSR_HD V3<F> sh_viewdir_vjp(const Cam<F>& cam, V3<F> mean, V3<F> vd, int degree,
 }
 
 // exact == false reproduces the reference approximations (see above);
+// hp selects the FP64 compensation and inversion of the forward's
+// high-precision conic mode;
 // sh_dir == false leaves out only the view-direction term even when exact
 // (callers that add sh_viewdir_vjp themselves).
 template <class F, class Coeff>
 GSR_HD ParamGrad<F> project_backward(const Cam<F>& cam, V3<F> mean, V4<F> quat_unorm, V3<F> log_scale, F raw_opac,
                                      F cov_blur, V2<F> v_xy, V3<F> v_conic, V3<F> v_color, F v_opac, int degree,
-                                     const Coeff& coeff, bool exact, bool sh_dir = true) {
+                                     const Coeff& coeff, bool exact, bool sh_dir = true, bool hp = false) {
   ParamGrad<F> g;
   const V3<F> vd = view_dir(cam, mean);
   g.viewdir = vd;
@@ -1008,10 +1010,18 @@ GSR_HD ParamGrad<F> project_backward(const Cam<F>& cam, V3<F> mean, V4<F> quat_u
   const M32<F> j = calc_cam_j(mc, cam);
   const M2<F> cov_start = mul(mul(j, cov_cam), transpose(j));
   M2<F> cov2d = cov_start;
-  const F fc = compensate_cov2d(cov2d, cov_blur);
+  const F fc = hp ? compensate_cov2d_hp(cov2d, cov_blur) : compensate_cov2d(cov2d, cov_blur);
   const F opac = sigmoid(raw_opac);
   g.v_raw_opac = fc * v_opac * opac * (F(1) - opac);
-  const M2<F> cinv = inverse2x2(cov2d);
+  M2<F> cinv;
+  {
+    // The conic the forward used (FP64 inversion in high-precision mode).
+    const V3<F> c = hp ? inverse2x2_packed_hp(cov2d) : inverse2x2_packed(cov2d);
+    cinv.m[0][0] = c.x;
+    cinv.m[0][1] = c.y;
+    cinv.m[1][0] = c.y;
+    cinv.m[1][1] = c.z;
+  }
   M2<F> vci;
   vci.m[0][0] = v_conic.x;
   vci.m[0][1] = F(0.5) * v_conic.y;

@@ -32,6 +32,7 @@ struct PairArgs {
   float cov_blur;
   FwdBufs b;
   int exact;
+  int hp;
 };
 
 struct NoCoeff {
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(128) pair_bwd_kernel(PairArgs a) {
     const ParamGrad<float> pg = project_backward(
         cam, V3<float>{t01.x, t01.y, t23.x}, V4<float>{t23.y, t45.x, t45.y, t67.x}, V3<float>{t67.y, t89.x, t89.y},
         a.sp.raw_opac[g], a.cov_blur, V2<float>{q0.x, q0.y}, V3<float>{q0.z, q0.w, q1.x}, V3<float>{q1.y, q1.z, q1.w},
-        q2.x, a.sp.degree, NoCoeff(), a.exact != 0, false);
+        q2.x, a.sp.degree, NoCoeff(), a.exact != 0, false, a.hp != 0);
     const size_t cap = a.b.Vcap;
     pair[0 * cap + c] = make_float4(pg.v_mean.x, pg.v_mean.y, pg.v_mean.z, pg.v_raw_opac);
     pair[1 * cap + c] = make_float4(pg.v_quat.x, pg.v_quat.y, pg.v_quat.z, pg.v_quat.w);
@@ -375,6 +376,7 @@ cudaError_t launch_project_bwd(const SplatsDev& sp, const ViewSet& vs, float cov
   pr.cov_blur = cov_blur;
   pr.b = b;
   pr.exact = pa.exact;
+  pr.hp = pa.hp;
   int px = num_sms * 16 / (int)vs.n_views;
   if (px < 1) px = 1;
   pair_bwd_kernel<<<dim3(px, vs.n_views), 128, 0, st>>>(pr);

@@ -572,14 +572,36 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   }
 }
 
+// Gaussians per shared-memory batch: 0 selects the tuned defaults (128 in
+// the forward, 64 in the backward); other values round up to 64, 128 or 256.
+// The backward of shapes with four warps per tile caps at 128 (its per-warp
+// partial sums would not fit the 48 KB of static shared memory).
+inline int pick_batch(uint32_t want, int dflt) {
+  if (want == 0) return dflt;
+  return want <= 64 ? 64 : (want <= 128 ? 128 : 256);
+}
+
 template <int TW, int TH, int PPL>
-cudaError_t launch_fwd_shape(const RasterArgs& a, uint32_t items, cudaStream_t st) {
-  raster_fwd_kernel<TW, TH, PPL, 128><<<items, TW * TH / PPL, 0, st>>>(a);
+cudaError_t launch_fwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
+  constexpr int NT = TW * TH / PPL;
+  switch (pick_batch(batch, 128)) {
+    case 64: raster_fwd_kernel<TW, TH, PPL, 64><<<items, NT, 0, st>>>(a); break;
+    case 128: raster_fwd_kernel<TW, TH, PPL, 128><<<items, NT, 0, st>>>(a); break;
+    default: raster_fwd_kernel<TW, TH, PPL, 256><<<items, NT, 0, st>>>(a); break;
+  }
   return cudaGetLastError();
 }
 template <int TW, int TH, int PPL>
-cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t items, cudaStream_t st) {
-  raster_bwd_kernel<TW, TH, PPL, 64><<<items, TW * TH / PPL, 0, st>>>(a);
+cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
+  constexpr int NT = TW * TH / PPL;
+  constexpr int kMaxBatch = NT / 32 >= 4 ? 128 : 256;
+  int b = pick_batch(batch, 64);
+  if (b > kMaxBatch) b = kMaxBatch;
+  switch (b) {
+    case 64: raster_bwd_kernel<TW, TH, PPL, 64><<<items, NT, 0, st>>>(a); break;
+    case 128: raster_bwd_kernel<TW, TH, PPL, 128><<<items, NT, 0, st>>>(a); break;
+    default: raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128)><<<items, NT, 0, st>>>(a); break;
+  }
   return cudaGetLastError();
 }
 
@@ -598,9 +620,9 @@ cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, fl
   cudaError_t e = cudaMemsetAsync(b.visible_c, 0, b.Vcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, kFwdPPL>(a, vs.total_tiles, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, kFwdPPL>(a, vs.total_tiles, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, kFwdPPL>(a, vs.total_tiles, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
   return cudaErrorInvalidValue;
 }
 
@@ -621,9 +643,9 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     if (e != cudaSuccess) return e;
   }
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.total_tiles, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.total_tiles, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.total_tiles, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.total_tiles, vs.batch, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.total_tiles, vs.batch, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.total_tiles, vs.batch, st);
   return cudaErrorInvalidValue;
 }
 

@@ -152,25 +152,30 @@ def config3_targets(seed_offset=0, n=1_000_000):
     return tr, sh, op
 
 
-def config4(seed_offset=0, n=3_000_000):
-    """Mixed precision: 3M Gaussians, 5% flattened (one log-scale -9), 1920x1080."""
+def config4(seed_offset=0, n=3_000_000, width=1920, height=1080):
+    """Mixed precision: 3M Gaussians, 5% flattened (one log-scale -9), 1920x1080
+    (fx = fy = 1400 at full width; scaled with the width for smaller cases)."""
     rng = np.random.Generator(np.random.PCG64(SEED_BASE + 3 + seed_offset))
     tr, sh, op = _gaussians(rng, n, 3, _blob_means(rng, n))
     flat = rng.random(n) < 0.05
     axis = rng.integers(0, 3, n)
     tr[np.nonzero(flat)[0], 7 + axis[flat]] = -9.0
-    cam = look_at(np.array([0.0, 0.0, -5.0]), (0, 0, 0), 1400, 1400, 959.5, 539.5, 1920, 1080)
+    f = 1400.0 * width / 1920.0
+    cam = look_at(np.array([0.0, 0.0, -5.0]), (0, 0, 0), f, f, (width - 1) / 2, (height - 1) / 2, width, height)
     return Scene(tr, sh, op, 3, [cam], "c4")
 
 
-def config5(seed_offset=0, n=2_000_000, views=32):
+C5_RESOLUTIONS = ((320, 240), (640, 480), (1280, 720), (1920, 1080))
+
+
+def config5(seed_offset=0, n=2_000_000, views=32, resolutions=C5_RESOLUTIONS):
     """Uneven batch: 32 views of mixed resolution at distances U[1.5, 8]."""
     rng = np.random.Generator(np.random.PCG64(SEED_BASE + 4 + seed_offset))
     tr, sh, op = _gaussians(rng, n, 3, _blob_means(rng, n))
-    res = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+    res = list(resolutions)
     cams = []
     for d in _sphere_dirs(rng, views):
-        w, h = res[int(rng.integers(0, 4))]
+        w, h = res[int(rng.integers(0, len(res)))]
         r = float(rng.uniform(1.5, 8.0))
         f = 0.8203125 * w
         cams.append(look_at(r * d, (0, 0, 0), f, f, (w - 1) / 2, (h - 1) / 2, w, h))

@@ -49,6 +49,8 @@ def test_struct_layouts_match_header():
         "gsr_adam_state": _lib.gsr_adam_state,
         "gsr_lr": _lib.gsr_lr,
         "gsr_train_params": _lib.gsr_train_params,
+        "gsr_tune_candidate": _lib.gsr_tune_candidate,
+        "gsr_tune_result": _lib.gsr_tune_result,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():

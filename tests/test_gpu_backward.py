@@ -3,8 +3,8 @@ sums and parameter gradients against the CPU oracle (relative 1e-4 with an
 absolute floor of 1e-3 x the largest reference value for entries that cancel),
 in the exact-adjoint and reference-semantics modes; deterministic mode is
 bitwise repeatable. Parameter gradients are checked with assert_grad_parity
-(norm-wise 1e-4 against the FP32 oracle, element-wise anchored on the FP64
-oracle)."""
+(norm-wise 1e-4 against the FP32 oracle, at least as accurate as the FP32
+oracle against the FP64 one, and an element-wise screen)."""
 import numpy as np
 import pytest
 
