@@ -201,7 +201,11 @@ def stage_profile(ctx, fn):
 
 
 def cpu_baseline(scene, cams, targets_np):
-    """Oracle (C++ restatement, OpenMP over all host threads) on one view of the workload."""
+    """CPU baselines on one view of the workload (a bounded sample, ~10-30 s):
+    the oracle (C++ restatement of the training path, forward + loss + exact
+    backward, OpenMP over all host threads) is the value; the reference's own
+    shipped CPU renderer (tiled_renderer.rs restated, forward only, one
+    thread, different semantics) is reported beside it."""
     from oracle import oracle as O
 
     cam = cams[0]
@@ -210,9 +214,15 @@ def cpu_baseline(scene, cams, targets_np):
     _, vp = O.loss(f.image, targets_np[0])
     f.backward(vp, mode=0)
     dt = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    O.ref_cpu_forward(scene, cam)
+    dt_ref = time.perf_counter() - t1
     return {"value": dt * 1000.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": "1 of the 8 views (1M Gaussians, 1280x720): oracle forward + loss + exact backward, "
-                      "OpenMP over all host threads"}
+                      "OpenMP over all host threads",
+            "reference_cpu_forward": {"value": dt_ref * 1000.0, "unit": UNIT, "cores": 1,
+                                      "sample": "the same view through the reference's shipped CPU renderer "
+                                                "(TiledRenderer, forward only, single-threaded as shipped)"}}
 
 
 def run_reference(args):

@@ -190,3 +190,27 @@ def densify(v_transforms, stats, v_sh, visible, acc, use_visible=False):
     n, K = v_sh.shape[0], v_sh.shape[1]
     args = [np.ascontiguousarray(a, dtype=np.float32) for a in (v_transforms, stats, v_sh, visible)]
     lib().orc_densify_f32(*[_p(a, f32p) for a in args], n, K, int(use_visible), _p(acc, f32p))
+
+
+def ref_cpu_forward(scene, cam, cov_blur=0.3, background=(0.0, 0.0, 0.0)):
+    """The reference's shipped single-threaded CPU renderer (tiled_renderer.rs,
+    restated in ref_cpu_forward.cpp): returns (colour [H,W,3], depth [H,W]).
+    Different semantics from the training path; timed only."""
+    L = lib()
+    f = L.orc_ref_cpu_forward
+    f.restype = None
+    tr = np.ascontiguousarray(scene.transforms, np.float32)
+    sh = np.ascontiguousarray(scene.sh, np.float32)
+    op = np.ascontiguousarray(scene.raw_opacity, np.float32)
+    vm = np.ascontiguousarray(cam.viewmat, np.float32)
+    cp = np.ascontiguousarray(cam.campos, np.float32)
+    bg = np.ascontiguousarray(background, np.float32)
+    col = np.zeros((cam.height, cam.width, 3), np.float32)
+    dep = np.zeros((cam.height, cam.width), np.float32)
+    fp = C.c_void_p
+    f(tr.ctypes.data_as(fp), sh.ctypes.data_as(fp), op.ctypes.data_as(fp), C.c_int(op.shape[0]),
+      C.c_int(scene.sh_degree), vm.ctypes.data_as(fp), cp.ctypes.data_as(fp), C.c_float(cam.fx), C.c_float(cam.fy),
+      C.c_float(cam.cx), C.c_float(cam.cy), C.c_int(cam.width), C.c_int(cam.height), C.c_float(cov_blur),
+      bg.ctypes.data_as(fp), col.ctypes.data_as(fp), dep.ctypes.data_as(fp))
+    return col, dep
+

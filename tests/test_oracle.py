@@ -235,3 +235,26 @@ def test_adam_matches_numpy_restatement():
         upd = (mr / bc1) / (np.sqrt(vr / bc2) + np.float32(1e-8))
         pr = pr - upd * np.tile(np.float32([0.01, 0.02]), 50)
     np.testing.assert_allclose(p, pr, rtol=1e-5, atol=1e-6)
+
+
+def test_reference_cpu_forward_single_splat():
+    """tiled_renderer/tests.rs:39-97 restated: one splat at (0,0,1), scale 0.01,
+    opacity 0.5, colour (1, 0.5, 0.25), 64x64, f=500, principal point (32,32):
+    it projects to the image centre with depth 1, blends its colour there, and
+    the output stays within [0, 1]."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from rustscan_b200 import scenes as S
+
+    tr = np.array([[0, 0, 1, 1, 0, 0, 0, np.log(0.01), np.log(0.01), np.log(0.01)]], np.float32)
+    rgb = np.array([1.0, 0.5, 0.25])
+    sh = ((rgb - 0.5) / S.SH_C0).reshape(1, 1, 3).astype(np.float32)
+    op = np.array([np.log(0.5 / 0.5)], np.float32)
+    cam = S.camera_from_rt(np.eye(3), np.zeros(3), 500, 500, 32, 32, 64, 64)
+    col, dep = O.ref_cpu_forward(S.Scene(tr, sh, op, 0, [cam]), cam)
+    assert dep[32, 32] == np.float32(1.0) or dep[31, 31] == np.float32(1.0)
+    c = col[31:33, 31:33].reshape(-1, 3).max(axis=0)
+    assert c[0] > 0.2 and abs(c[1] / c[0] - 0.5) < 1e-3 and abs(c[2] / c[0] - 0.25) < 1e-3
+    assert col.min() >= 0.0 and col.max() <= 1.0
+    assert np.all(dep[0, 0] == np.float32(np.finfo(np.float32).max))
