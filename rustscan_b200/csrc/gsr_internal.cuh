@@ -98,22 +98,38 @@ __device__ __forceinline__ uint32_t lookback(unsigned long long* states, uint32_
     return 0;
   }
   st_volatile64(states + (size_t)part * stride, tag | kFlagAgg | agg);
+  // Walk back over the predecessors kLookbackWindow states per round trip:
+  // the window's loads are independent and in flight together; the states
+  // are then consumed in order up to the first inclusive prefix (done) or
+  // the first predecessor that has not published yet (poll again from it).
+  constexpr int kLookbackWindow = 8;
   uint32_t sum = 0;
   int64_t j = (int64_t)part - 1;
   uint32_t polls = 0;
-  while (j >= 0) {
-    const unsigned long long s = ld_volatile64(states + (size_t)j * stride);
-    if ((s >> 34) != (tag >> 34) || ((s >> 32) & 3ull) == 0) {
+  bool done = false;
+  while (j >= 0 && !done) {
+    unsigned long long w[kLookbackWindow];
+#pragma unroll
+    for (int k = 0; k < kLookbackWindow; ++k) w[k] = j - k >= 0 ? ld_volatile64(states + (size_t)(j - k) * stride) : 0ull;
+    int used = 0;
+#pragma unroll
+    for (int k = 0; k < kLookbackWindow; ++k) {
+      if (done || used < k || j - k < 0) continue;
+      const unsigned long long s = w[k];
+      if ((s >> 34) != (tag >> 34) || ((s >> 32) & 3ull) == 0) continue;  // not published: stop consuming
+      sum += (uint32_t)s;
+      used = k + 1;
+      if (((s >> 32) & 3ull) == 2ull) done = true;
+    }
+    j -= used;
+    if (!done && used < kLookbackWindow && j >= 0) {
+      // Stopped at an unpublished predecessor.
       if (++polls > kMaxPolls) {
         report_timeout(status, where);
         break;
       }
-      __nanosleep(20);
-      continue;
+      if (used == 0) __nanosleep(20);
     }
-    sum += (uint32_t)s;
-    if (((s >> 32) & 3ull) == 2ull) break;
-    --j;
   }
   st_volatile64(states + (size_t)part * stride, tag | kFlagPre | (uint32_t)(sum + agg));
   return sum;

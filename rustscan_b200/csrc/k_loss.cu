@@ -6,7 +6,7 @@
 // C2 = 9e-4 and denominators clamped at 1e-8. The reference builds it from
 // ~10 burn ops and differentiates through burn autodiff; here two tiled
 // kernels do the work:
-//  pass 1: per 32x16 output tile and channel, the five blurred moments in
+//  pass 1: per 32x32 output tile and channel, the five blurred moments in
 //          shared memory, the SSIM map, its partial derivatives with respect
 //          to (mu_x, E[x^2], E[xy]) and per-tile partial sums of SSIM and L1;
 //  pass 2: the adjoint of the padded separable blur applied to the three
@@ -18,7 +18,7 @@ namespace gsr {
 
 namespace {
 
-constexpr int LTX = 32, LTY = 16, R = 5, WIN = 11;
+constexpr int LTX = 32, LTY = 32, R = 5, WIN = 11;
 constexpr int HX = LTX + 2 * R, HY = LTY + 2 * R;
 
 struct LossArgs {
@@ -35,11 +35,23 @@ struct LossArgs {
 };
 
 __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// Pass 1. Shared memory holds the five input planes (x, y, x^2, y^2, xy) of
+// the replicate-padded halo, then the horizontally blurred planes. Each
+// thread blurs two adjacent columns at once with paired FP32 arithmetic,
+// sliding one load per tap along the row (horizontal) or down the column
+// pair (vertical, two output rows per thread).
+struct SsimFwdSmem {
+  float p[5][HY][HX];
+  float h[5][HY][LTX];
+  float red[2][8];
+};
 
 __global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
-  __shared__ float s_x[HY][HX], s_y[HY][HX];
-  __shared__ float s_h[5][HY][LTX];
-  __shared__ float s_red[2][8];
+  extern __shared__ float4 smem_raw[];
+  SsimFwdSmem& S = *reinterpret_cast<SsimFwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
   const ViewDesc& vd = a.views[v];
   const int W = (int)vd.w, H = (int)vd.h;
@@ -53,63 +65,78 @@ __global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
     const int hy = i / HX, hx = i % HX;
     const int gx = clampi(x0 + hx - R, 0, W - 1), gy = clampi(y0 + hy - R, 0, H - 1);
     const size_t p = (size_t)gy * W + gx;
-    s_x[hy][hx] = pred[p * 4 + ch];
-    s_y[hy][hx] = tgt[p * 3 + ch];
+    const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
+    S.p[0][hy][hx] = x;
+    S.p[1][hy][hx] = y;
+    S.p[2][hy][hx] = x * x;
+    S.p[3][hy][hx] = y * y;
+    S.p[4][hy][hx] = x * y;
   }
   __syncthreads();
-  // Horizontal pass for all halo rows.
-  for (int i = threadIdx.x; i < HY * LTX; i += blockDim.x) {
-    const int hy = i / LTX, ox = i % LTX;
-    float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f, m4 = 0.f;
+  // Horizontal pass: every halo row, output columns in pairs.
+  for (int i = threadIdx.x; i < HY * (LTX / 2); i += blockDim.x) {
+    const int hy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
 #pragma unroll
-    for (int t = 0; t < WIN; ++t) {
-      const float xv = s_x[hy][ox + t], yv = s_y[hy][ox + t], w = a.k[t];
-      m0 = m0 + w * xv;
-      m1 = m1 + w * yv;
-      m2 = m2 + w * (xv * xv);
-      m3 = m3 + w * (yv * yv);
-      m4 = m4 + w * (xv * yv);
+    for (int m = 0; m < 5; ++m) {
+      const float* row = &S.p[m][hy][ox];
+      float2 acc = f2(0.f);
+      float prev = row[0];
+#pragma unroll
+      for (int t = 0; t < WIN; ++t) {
+        const float next = row[t + 1];
+        acc = fma2(f2(a.k[t]), make_float2(prev, next), acc);
+        prev = next;
+      }
+      *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc;
     }
-    s_h[0][hy][ox] = m0;
-    s_h[1][hy][ox] = m1;
-    s_h[2][hy][ox] = m2;
-    s_h[3][hy][ox] = m3;
-    s_h[4][hy][ox] = m4;
   }
   __syncthreads();
+  // Vertical pass and the SSIM map: a column pair times two rows per thread.
   const float C1 = 1e-4f, C2 = 9e-4f;
   float ssum = 0.f, lsum = 0.f;
   float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
-  for (int i = threadIdx.x; i < LTX * LTY; i += blockDim.x) {
-    const int oy = i / LTX, ox = i % LTX;
-    const int gx = x0 + ox, gy = y0 + oy;
-    if (gx >= W || gy >= H) continue;
-    float mx = 0.f, my = 0.f, exx = 0.f, eyy = 0.f, exy = 0.f;
+  {
+    const int ox = 2 * (threadIdx.x % (LTX / 2)), oy = 2 * (threadIdx.x / (LTX / 2));  // 16 x 16 tasks
+    float2 mo[5][2];
 #pragma unroll
-    for (int t = 0; t < WIN; ++t) {
-      const float w = a.k[t];
-      mx = mx + w * s_h[0][oy + t][ox];
-      my = my + w * s_h[1][oy + t][ox];
-      exx = exx + w * s_h[2][oy + t][ox];
-      eyy = eyy + w * s_h[3][oy + t][ox];
-      exy = exy + w * s_h[4][oy + t][ox];
+    for (int m = 0; m < 5; ++m) {
+      float2 r0 = f2(0.f), r1 = f2(0.f);
+      float2 prev = *reinterpret_cast<const float2*>(&S.h[m][oy][ox]);
+#pragma unroll
+      for (int t = 0; t < WIN; ++t) {
+        const float2 next = *reinterpret_cast<const float2*>(&S.h[m][oy + t + 1][ox]);
+        r0 = fma2(f2(a.k[t]), prev, r0);
+        r1 = fma2(f2(a.k[t]), next, r1);
+        prev = next;
+      }
+      mo[m][0] = r0;
+      mo[m][1] = r1;
     }
-    const float sxx = exx - mx * mx, syy = eyy - my * my, sxy = exy - mx * my;
-    const float A = 2.f * mx * my + C1, B = 2.f * sxy + C2;
-    const float Cr = mx * mx + my * my + C1, Dr = sxx + syy + C2;
-    const float Cc = fmaxf(Cr, 1e-8f), Dc = fmaxf(Dr, 1e-8f);
-    const float s = (A * B) / (Cc * Dc);
-    const float inv = 1.f / (Cc * Dc);
-    const float dC = Cr > 1e-8f ? 1.f : 0.f, dD = Dr > 1e-8f ? 1.f : 0.f;
-    const float gmx = (2.f * my * B + A * (-2.f * my)) * inv - s * ((2.f * mx * dC) * Dc + Cc * (-2.f * mx * dD)) / (Cc * Dc);
-    const float gexx = -s * dD / Dc;
-    const float gexy = 2.f * A * inv;
-    const size_t p = (size_t)gy * W + gx;
-    maps[p] = gmx;
-    maps[a.Pcap + p] = gexx;
-    maps[2 * a.Pcap + p] = gexy;
-    ssum += s;
-    lsum += fabsf(s_x[oy + R][ox + R] - s_y[oy + R][ox + R]);
+#pragma unroll
+    for (int ry = 0; ry < 2; ++ry) {
+#pragma unroll
+      for (int cx = 0; cx < 2; ++cx) {
+        const int gx = x0 + ox + cx, gy = y0 + oy + ry;
+        if (gx >= W || gy >= H) continue;
+        const float mx = cx ? mo[0][ry].y : mo[0][ry].x, my = cx ? mo[1][ry].y : mo[1][ry].x;
+        const float exx = cx ? mo[2][ry].y : mo[2][ry].x, eyy = cx ? mo[3][ry].y : mo[3][ry].x;
+        const float exy = cx ? mo[4][ry].y : mo[4][ry].x;
+        const float sxx = exx - mx * mx, syy = eyy - my * my, sxy = exy - mx * my;
+        const float A = 2.f * mx * my + C1, B = 2.f * sxy + C2;
+        const float Cr = mx * mx + my * my + C1, Dr = sxx + syy + C2;
+        const float Cc = fmaxf(Cr, 1e-8f), Dc = fmaxf(Dr, 1e-8f);
+        const float inv = 1.f / (Cc * Dc);
+        const float s = (A * B) * inv;
+        const float dC = Cr > 1e-8f ? 1.f : 0.f, dD = Dr > 1e-8f ? 1.f : 0.f;
+        const float gmx = (2.f * my * B + A * (-2.f * my)) * inv - s * ((2.f * mx * dC) * Dc + Cc * (-2.f * mx * dD)) * inv;
+        const size_t p = (size_t)gy * W + gx;
+        maps[p] = gmx;
+        maps[a.Pcap + p] = -s * dD / Dc;
+        maps[2 * a.Pcap + p] = 2.f * A * inv;
+        ssum += s;
+        lsum += fabsf(S.p[0][oy + ry + R][ox + cx + R] - S.p[1][oy + ry + R][ox + cx + R]);
+      }
+    }
   }
   // Fixed-order block reduction.
   for (int o = 16; o > 0; o >>= 1) {
@@ -117,15 +144,15 @@ __global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
     lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    s_red[0][threadIdx.x >> 5] = ssum;
-    s_red[1][threadIdx.x >> 5] = lsum;
+    S.red[0][threadIdx.x >> 5] = ssum;
+    S.red[1][threadIdx.x >> 5] = lsum;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     float a0 = 0.f, a1 = 0.f;
     for (int w = 0; w < 8; ++w) {
-      a0 += s_red[0][w];
-      a1 += s_red[1][w];
+      a0 += S.red[0][w];
+      a1 += S.red[1][w];
     }
     float* pp = a.partial + (((size_t)v * 3 + ch) * a.tiles_cap + tile) * 2;
     pp[0] = a0;
@@ -134,7 +161,8 @@ __global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
 }
 
 // Weight of output q in the adjoint of a replicate-padded 11-tap
-// correlation at input p along an axis of length n.
+// correlation at input p along an axis of length n (k is symmetric, so for
+// interior p it is k[R + q - p]; the border inputs collect the clamped taps).
 __device__ __forceinline__ float adj_weight(const float* k, int p, int q, int n) {
   if (p > 0 && p < n - 1) {
     const int d = q - p;
@@ -147,9 +175,18 @@ __device__ __forceinline__ float adj_weight(const float* k, int p, int q, int n)
   return w;
 }
 
+// Pass 2: the adjoint of the padded separable blur on the three partial
+// maps (vertical, then horizontal), combined with the L1 sign. Interior
+// rows and column pairs take the symmetric-kernel fast path with paired
+// arithmetic; rows and columns on the image border use adj_weight.
+struct SsimBwdSmem {
+  float g[3][HY][HX];
+  float v[3][LTY][HX];
+};
+
 __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
-  __shared__ float s_g[3][HY][HX];
-  __shared__ float s_v[3][LTY][HX];
+  extern __shared__ float4 smem_raw[];
+  SsimBwdSmem& S = *reinterpret_cast<SsimBwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
   const ViewDesc& vd = a.views[v];
   const int W = (int)vd.w, H = (int)vd.h;
@@ -164,25 +201,28 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
     const bool ok = gx >= 0 && gx < W && gy >= 0 && gy < H;
     const size_t p = (size_t)gy * W + gx;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) s_g[m][hy][hx] = ok ? maps[m * a.Pcap + p] : 0.f;
+    for (int m = 0; m < 3; ++m) S.g[m][hy][hx] = ok ? maps[m * a.Pcap + p] : 0.f;
   }
   __syncthreads();
-  // Adjoint of the vertical pass: rows of the tile, all halo columns.
-  for (int i = threadIdx.x; i < LTY * HX; i += blockDim.x) {
-    const int oy = i / HX, hx = i % HX;
+  // Adjoint of the vertical pass: tile rows, all halo columns (in pairs).
+  for (int i = threadIdx.x; i < LTY * (HX / 2); i += blockDim.x) {
+    const int oy = i / (HX / 2), hx = 2 * (i % (HX / 2));
     const int py = y0 + oy;
-    float acc[3] = {0.f, 0.f, 0.f};
+    float2 acc[3] = {f2(0.f), f2(0.f), f2(0.f)};
     if (py < H) {
+      const bool interior = py > 0 && py < H - 1;
+#pragma unroll
       for (int d = -R; d <= R; ++d) {
         const int qy = py + d;
-        if (qy < 0 || qy >= H) continue;
-        const float w = adj_weight(a.k, py, qy, H);
+        if (qy < 0 || qy >= H) continue;  // zero rows outside the image
+        const float w = interior ? a.k[R + d] : adj_weight(a.k, py, qy, H);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) acc[m] = acc[m] + w * s_g[m][oy + R + d][hx];
+        for (int m = 0; m < 3; ++m)
+          acc[m] = fma2(f2(w), *reinterpret_cast<const float2*>(&S.g[m][oy + R + d][hx]), acc[m]);
       }
     }
 #pragma unroll
-    for (int m = 0; m < 3; ++m) s_v[m][oy][hx] = acc[m];
+    for (int m = 0; m < 3; ++m) *reinterpret_cast<float2*>(&S.v[m][oy][hx]) = acc[m];
   }
   __syncthreads();
   const float* pred = a.pred + vd.pix_base * 4;
@@ -190,24 +230,52 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
   float* out = a.v_pred + vd.pix_base * 4;
   const float M = 3.f * (float)W * (float)H;
   const float kl = a.l1_w / M, ks = -a.ssim_w / M;
-  for (int i = threadIdx.x; i < LTX * LTY; i += blockDim.x) {
-    const int oy = i / LTX, ox = i % LTX;
+  for (int i = threadIdx.x; i < LTY * (LTX / 2); i += blockDim.x) {
+    const int oy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
     const int px = x0 + ox, py = y0 + oy;
     if (px >= W || py >= H) continue;
-    float acc[3] = {0.f, 0.f, 0.f};
-    for (int d = -R; d <= R; ++d) {
-      const int qx = px + d;
-      if (qx < 0 || qx >= W) continue;
-      const float w = adj_weight(a.k, px, qx, W);
+    float2 acc[3] = {f2(0.f), f2(0.f), f2(0.f)};
+    if (px > 0 && px + 1 < W - 1) {
+      // Both columns interior: the symmetric kernel, paired.
 #pragma unroll
-      for (int m = 0; m < 3; ++m) acc[m] = acc[m] + w * s_v[m][oy][ox + R + d];
+      for (int d = -R; d <= R; ++d) {
+        const float w = a.k[R + d];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+          acc[m] = fma2(f2(w), make_float2(S.v[m][oy][ox + R + d], S.v[m][oy][ox + 1 + R + d]), acc[m]);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int pc = px + c;
+        if (pc >= W) continue;
+        float s3[3] = {0.f, 0.f, 0.f};
+        for (int d = -R; d <= R; ++d) {
+          const int qx = pc + d;
+          if (qx < 0 || qx >= W) continue;
+          const float w = adj_weight(a.k, pc, qx, W);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) s3[m] = s3[m] + w * S.v[m][oy][ox + c + R + d];
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          if (c) acc[m].y = s3[m];
+          else acc[m].x = s3[m];
+        }
+      }
     }
-    const size_t p = (size_t)py * W + px;
-    const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
-    const float dlt = x - y;
-    const float sg = dlt > 0.f ? 1.f : (dlt < 0.f ? -1.f : 0.f);
-    out[p * 4 + ch] = kl * sg + ks * (acc[0] + 2.f * x * acc[1] + y * acc[2]);
-    if (ch == 0) out[p * 4 + 3] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int pc = px + c;
+      if (pc >= W) continue;
+      const float a0 = c ? acc[0].y : acc[0].x, a1 = c ? acc[1].y : acc[1].x, a2 = c ? acc[2].y : acc[2].x;
+      const size_t p = (size_t)py * W + pc;
+      const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
+      const float dlt = x - y;
+      const float sg = dlt > 0.f ? 1.f : (dlt < 0.f ? -1.f : 0.f);
+      out[p * 4 + ch] = kl * sg + ks * (a0 + 2.f * x * a1 + y * a2);
+      if (ch == 0) out[p * 4 + 3] = 0.f;
+    }
   }
 }
 
@@ -284,8 +352,11 @@ cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const flo
   a.ssim_w = ssim_w;
   if (tmax == 0) return cudaSuccess;
   dim3 grid(tmax, 3, vs.n_views);
-  ssim_fwd_kernel<<<grid, 256, 0, st>>>(a);
-  ssim_bwd_kernel<<<grid, 256, 0, st>>>(a);
+  // More than the 48 KB default of dynamic shared memory (set for the current device).
+  cudaFuncSetAttribute(ssim_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SsimFwdSmem));
+  cudaFuncSetAttribute(ssim_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SsimBwdSmem));
+  ssim_fwd_kernel<<<grid, 256, sizeof(SsimFwdSmem), st>>>(a);
+  ssim_bwd_kernel<<<grid, 256, sizeof(SsimBwdSmem), st>>>(a);
   loss_reduce_kernel<<<vs.n_views, 256, 0, st>>>(a, vs.n_views, loss);
   return cudaGetLastError();
 }
