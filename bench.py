@@ -358,8 +358,21 @@ def main():
     }
     dom = max((k for k in algo), key=lambda k: stages.get(k, 0.0))
     achieved = algo[dom] / (stages[dom] * 1e-3) / 1e9
+    # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
+    # capture of a single 1280x720 view of this workload (6,273,269
+    # intersections), scaled to the launch by its intersections (the raster
+    # and tile-sort traffic grows with them) or, for Adam, taken as is (it
+    # sweeps the N parameters once per step).
+    traffic_coeff = {"raster_bwd": (38.71e6 + 0.035e6) / 6273269, "raster_fwd": (14.12e6 + 0.25e6) / 6273269,
+                     "tile_sort": (52.6e6 + 6.0e6 + 52.4e6 + 7.0e6) / 6273269}
+    if dom in traffic_coeff:
+        traffic = traffic_coeff[dom] * sum(I)
+    elif dom == "adam":
+        traffic = (160.0e6 + 63.1e6 + 768.0e6 + 520.4e6 + 16.0e6) * args.n / 1_000_000
+    else:
+        traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes": algo[dom], "launch_ms": stages[dom]}
 
     # ---- plain single-view path (one view per call, FP32, no graph) ------------
