@@ -2,10 +2,10 @@
 //
 // One thread per Gaussian evaluates every view of the launch: the
 // parameters are read once (the block stages its 256 x 40-byte transform
-// rows in shared memory with 128-bit loads), then for each view the thread
-// projects the Gaussian (project_forward.wgsl:19-96, project_visible.wgsl:
+// rows in shared memory with 128-bit loads), the thread projects the
+// Gaussian in every view (project_forward.wgsl:19-96, project_visible.wgsl:
 // 233-310) and the block compacts the visible ones in global-id order with a
-// decoupled look-back. The tiles each visible Gaussian touches are counted
+// decoupled look-back per view, all views' look-backs at once. The tiles each visible Gaussian touches are counted
 // afterwards by the warp-cooperative walk over the compact records. This replaces the
 // atomic compaction of project_forward.wgsl:94-96 (nondeterministic order)
 // and fuses the separate project_visible pass.
@@ -38,15 +38,20 @@ struct ProjectArgs {
 
 template <class SHT, int DEG>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
+  constexpr int kWarps = kProjThreads / 32;
   __shared__ float4 s_tr4[kProjThreads * 10 / 4];
-  __shared__ uint32_t s_scan[32];
-  __shared__ uint32_t s_part, s_excl;
+  __shared__ uint32_t s_mask[kMaxViews][kWarps];  // visibility ballots per view and warp
+  __shared__ uint32_t s_wpre[kMaxViews][kWarps];  // exclusive prefix over the warps
+  __shared__ uint32_t s_excl[kMaxViews];          // the partition's first compact index per view
+  __shared__ uint32_t s_part;
   const uint32_t epoch = epoch_begin(a.ctl);
   const uint32_t part = next_ticket(a.ctl, 0, &s_part);
   const uint32_t n = a.sp.n;
+  const uint32_t nv = a.vs.n_views;
   const uint32_t g0 = part * kProjThreads;
   const uint32_t g = g0 + threadIdx.x;
   const bool valid = g < n;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   float* s_tr = reinterpret_cast<float*>(s_tr4);
   // Stage this block's transform rows: 256 * 10 floats, 16-byte aligned.
   {
@@ -71,25 +76,46 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
     ls = V3<float>{t[7], t[8], t[9]};
     raw = __ldg(a.sp.raw_opac + g);
   }
-  const SHT* sh = reinterpret_cast<const SHT*>(a.sp.sh);
-  constexpr int K = (DEG + 1) * (DEG + 1);
   const TileShape ts{a.vs.tile_w, a.vs.tile_h};
-  for (uint32_t v = 0; v < a.vs.n_views; ++v) {
+  // Phase 1: visibility in every view; the block's per-view counts are
+  // published together and the views' look-backs run in parallel (thread v
+  // resolves view v), so the block waits once instead of once per view.
+  for (uint32_t v = 0; v < nv; ++v) {
     const ViewDesc& vd = a.vs.views[v];
     const Cam<float> cam = cam_from_desc<float>(vd);
-    Projected<float> p;
-    p.visible = false;
-    if (valid) p = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
-    uint32_t tot;
-    const uint32_t rank = block_exclusive_scan(p.visible ? 1u : 0u, s_scan, &tot);
-    if (threadIdx.x == 0) {
-      s_excl = lookback(a.states + (size_t)v * a.parts, 1, part, tot, epoch, a.status, kWaitCompact);
-      if (part == a.parts - 1) a.b.vcount[v * 4 + 0] = s_excl + tot;
+    bool vis = false;
+    if (valid) vis = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0).visible;
+    const uint32_t m = __ballot_sync(0xffffffffu, vis);
+    if (lane == 0) s_mask[v][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    const uint32_t v = threadIdx.x;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      s_wpre[v][w] = tot;
+      tot += (uint32_t)__popc(s_mask[v][w]);
     }
-    __syncthreads();
-    const uint32_t c = s_excl + rank;
-    if (valid) slice(a.b.c_of_gid, a.b.Ncap, v)[g] = p.visible ? (int32_t)c : -1;
-    if (p.visible) {
+    const uint32_t excl = lookback(a.states + (size_t)v * a.parts, 1, part, tot, epoch, a.status, kWaitCompact);
+    s_excl[v] = excl;
+    if (part == a.parts - 1) a.b.vcount[v * 4 + 0] = excl + tot;
+  }
+  __syncthreads();
+  // Phase 2: the visible Gaussians' records at their compact indices (the
+  // projection is recomputed: the same expression on the same inputs).
+  const SHT* sh = reinterpret_cast<const SHT*>(a.sp.sh);
+  constexpr int K = (DEG + 1) * (DEG + 1);
+  for (uint32_t v = 0; v < nv; ++v) {
+    const uint32_t m = s_mask[v][warp];
+    const bool vis = (m >> lane) & 1u;
+    const uint32_t c = s_excl[v] + s_wpre[v][warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    if (valid) slice(a.b.c_of_gid, a.b.Ncap, v)[g] = vis ? (int32_t)c : -1;
+    if (vis) {
+      const ViewDesc& vd = a.vs.views[v];
+      const Cam<float> cam = cam_from_desc<float>(vd);
+      const Projected<float> p =
+          project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
       const SHT* shg = sh + (size_t)g * K * 3;
       auto coeff = [&](int k, int ch) { return load_sh(shg, k * 3 + ch); };
       const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, mean), coeff);
