@@ -254,6 +254,42 @@ GSR_API gsr_status gsr_train_step(gsr_ctx* ctx, float* transforms, void* sh, flo
                           const float* targets, const gsr_train_params* params, float* densify_acc, float* loss,
                           int32_t use_graph, void* stream);
 
+/* ---- topology (RustGS/src/training/topology/apply.rs) -------------------- */
+/* A topology plan row: the output splat copies splat `source`, as is
+ * (GSR_TOPO_EXISTING) or as one half of a split, moved by -offset
+ * (GSR_TOPO_REFINE_EXISTING) or +offset (GSR_TOPO_REFINE_NEW), where offset
+ * is the source's scale times sample_scalar rotated by its quaternion; split
+ * halves have their largest scale axis halved and opacity 1 - sqrt(1 - o).
+ * Mirrors TopologyPlanRow (topology/mod.rs:831-843). */
+enum { GSR_TOPO_EXISTING = 0, GSR_TOPO_REFINE_EXISTING = 1, GSR_TOPO_REFINE_NEW = 2 };
+typedef struct gsr_topo_row {
+  uint32_t source;
+  int32_t kind;
+  float sample_scalar;
+  uint32_t _pad;
+} gsr_topo_row;
+/* Plan-wide options (TopologyMutationPlan::refine_decay and the opacity-reset
+ * aftermath; topology/mod.rs:776-780, 863-870). */
+typedef struct gsr_topo_params {
+  int32_t has_refine_decay;
+  float scale_decay, opacity_decay, train_t;
+  int32_t opacity_reset;
+  float opacity_reset_cap; /* 0.01 in the reference (LITEGS_OPACITY_RESET_CAP) */
+} gsr_topo_params;
+
+/* Builds the mutated splat set on the device: output row i from rows[i]
+ * (rows in device memory, m of them; pruning is a source that no row
+ * names). Writes dst_transforms [m,10], dst_sh [m,K,3] (same storage type as
+ * src) and dst_raw_opacity [m]; the destinations may not alias the source.
+ * Replaces apply_mutations (topology/apply.rs:10-27) with its host round
+ * trip (topology/bridge.rs:25-146). A row whose source is out of range is
+ * reported by gsr_sync_status as GSR_ERR_INVALID_ARG. Adam moments and the
+ * densification accumulators are the caller's to reset, as the reference
+ * resets them on topology changes (engine/trainer.rs:851-853). */
+GSR_API gsr_status gsr_topology_apply(gsr_ctx* ctx, const gsr_splats* src, const gsr_topo_row* rows, uint32_t m,
+                                      const gsr_topo_params* params, float* dst_transforms, void* dst_sh,
+                                      float* dst_raw_opacity, void* stream);
+
 /* ---- autotuner (no counterpart in the reference) ------------------------ */
 /* Candidates: tile shapes 16x16, 8x8, 32x8 times raster batches 64, 128,
  * 256 (9 entries, in that order). */

@@ -722,6 +722,37 @@ ORC_EXPORT void orc_adam_f32(float* p, const float* g, float* m, float* v, uint6
 // acc is 9 arrays of n floats: grad_2d, screen_grad_2d, abs_grad_2d,
 // abs_pixel_grad_2d, pixel_coverage, camera_depth, grad_color,
 // num_observations, visible_observations.
+// topology/apply.rs:29-94 restated through the shared topo_mutate: output
+// row i copies source rows[i*3] with kind rows[i*3+1] and sample scalar
+// (bits) rows[i*3+2]; SH rows are copied (sh_elems floats each).
+ORC_EXPORT int orc_topology_apply_f32(const float* tr, const float* sh, const float* op, uint32_t n, uint32_t sh_elems,
+                                      const uint32_t* rows, uint32_t m, int has_decay, float scale_decay,
+                                      float opacity_decay, float train_t, int opacity_reset, float reset_cap,
+                                      float* otr, float* osh, float* oop) {
+  TopoParams p{};
+  p.has_decay = has_decay;
+  p.scale_decay = scale_decay;
+  p.opacity_decay = opacity_decay;
+  p.train_t = train_t;
+  p.opacity_reset = opacity_reset;
+  p.reset_cap = reset_cap;
+  for (uint32_t i = 0; i < m; ++i) {
+    const uint32_t src = rows[(size_t)i * 3];
+    const int kind = (int)rows[(size_t)i * 3 + 1];
+    float sample;
+    memcpy(&sample, &rows[(size_t)i * 3 + 2], 4);
+    if (src >= n) return -1;
+    float t[10];
+    for (int k = 0; k < 10; ++k) t[k] = tr[(size_t)src * 10 + k];
+    float logit = op[src];
+    topo_mutate(t, logit, kind, sample, p);
+    for (int k = 0; k < 10; ++k) otr[(size_t)i * 10 + k] = t[k];
+    oop[i] = logit;
+    for (uint32_t k = 0; k < sh_elems; ++k) osh[(size_t)i * sh_elems + k] = sh[(size_t)src * sh_elems + k];
+  }
+  return 0;
+}
+
 ORC_EXPORT void orc_densify_f32(const float* v_tr, const float* stats, const float* v_sh, const float* visible,
                                 int n, int K, int use_visible, float* acc) {
   for (int i = 0; i < n; ++i) {

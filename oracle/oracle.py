@@ -214,3 +214,34 @@ def ref_cpu_forward(scene, cam, cov_blur=0.3, background=(0.0, 0.0, 0.0)):
       bg.ctypes.data_as(fp), col.ctypes.data_as(fp), dep.ctypes.data_as(fp))
     return col, dep
 
+
+def topology_apply(transforms, sh, raw_opacity, rows, has_decay=False, scale_decay=0.0, opacity_decay=0.0,
+                   train_t=0.0, opacity_reset=False, reset_cap=0.01):
+    """topology/apply.rs restated: rows is a sequence of (source, kind,
+    sample_scalar); returns (transforms [m,10], sh [m,K,3], raw_opacity [m])."""
+    L = lib()
+    f = L.orc_topology_apply_f32
+    f.restype = C.c_int
+    tr = np.ascontiguousarray(transforms, np.float32)
+    shf = np.ascontiguousarray(sh, np.float32)
+    op = np.ascontiguousarray(raw_opacity, np.float32)
+    n = op.shape[0]
+    m = len(rows)
+    rr = np.zeros((m, 3), np.uint32)
+    for i, (src, kind, sample) in enumerate(rows):
+        rr[i, 0] = src
+        rr[i, 1] = kind
+        rr[i, 2] = np.float32(sample).view(np.uint32)
+    elems = int(np.prod(shf.shape[1:])) if shf.ndim > 1 else 0
+    otr = np.zeros((m, 10), np.float32)
+    osh = np.zeros((m,) + shf.shape[1:], np.float32)
+    oop = np.zeros(m, np.float32)
+    fp = C.c_void_p
+    st = f(tr.ctypes.data_as(fp), shf.ctypes.data_as(fp), op.ctypes.data_as(fp), C.c_uint32(n), C.c_uint32(elems),
+           rr.ctypes.data_as(fp), C.c_uint32(m), C.c_int(int(has_decay)), C.c_float(scale_decay),
+           C.c_float(opacity_decay), C.c_float(train_t), C.c_int(int(opacity_reset)), C.c_float(reset_cap),
+           otr.ctypes.data_as(fp), osh.ctypes.data_as(fp), oop.ctypes.data_as(fp))
+    if st != 0:
+        raise ValueError("a plan row names a source out of range")
+    return otr, osh, oop
+

@@ -387,6 +387,85 @@ class AdamScaled:
             splats.num_splats(), splats.sh_degree, C.byref(gs), C.byref(st), C.byref(lr), self.step, _stream()))
 
 
+@dataclasses.dataclass
+class TopologyPlan:
+    """A topology mutation plan (TopologyMutationPlan, topology/mod.rs:831-870):
+    one row per output splat, (source index, kind, sample scalar) with kind one
+    of EXISTING, REFINE_EXISTING, REFINE_NEW; pruned splats are the sources no
+    row names. refine_decay is (opacity_decay, scale_decay, train_t) or None."""
+
+    EXISTING = _lib.GSR_TOPO_EXISTING
+    REFINE_EXISTING = _lib.GSR_TOPO_REFINE_EXISTING
+    REFINE_NEW = _lib.GSR_TOPO_REFINE_NEW
+    rows: list
+    refine_decay: tuple | None = None
+    opacity_reset: bool = False
+    opacity_reset_cap: float = 0.01  # LITEGS_OPACITY_RESET_CAP (topology/mod.rs:25)
+
+
+def apply_topology(ctx: Context, splats: DeviceSplats, plan: TopologyPlan, check=True) -> DeviceSplats:
+    """apply_mutations (topology/apply.rs:10-27) on the device: returns the
+    mutated splat set as new tensors; the input is unchanged. Adam moments and
+    densification accumulators are the caller's to reset, as the reference
+    does after a topology change."""
+    m = len(plan.rows)
+    rows = (_lib.gsr_topo_row * max(m, 1))()
+    for i, (src, kind, sample) in enumerate(plan.rows):
+        rows[i] = _lib.gsr_topo_row(int(src), int(kind), float(sample), 0)
+    d_rows = torch.frombuffer(bytearray(rows), dtype=torch.uint8)[: 16 * m].to("cuda") if m else None
+    p = _lib.gsr_topo_params()
+    if plan.refine_decay is not None:
+        p.has_refine_decay = 1
+        p.opacity_decay, p.scale_decay, p.train_t = (float(v) for v in plan.refine_decay)
+    p.opacity_reset = int(bool(plan.opacity_reset))
+    p.opacity_reset_cap = float(plan.opacity_reset_cap)
+    K = (splats.sh_degree + 1) ** 2
+    out = DeviceSplats(torch.empty((m, 10), dtype=torch.float32, device="cuda"),
+                       torch.empty((m, K, 3), dtype=splats.sh_coeffs.dtype, device="cuda"),
+                       torch.empty(m, dtype=torch.float32, device="cuda"), splats.sh_degree)
+    if m == 0:
+        return out
+    sp = splats.struct()
+    ctx._check(ctx._lib.gsr_topology_apply(ctx._h, C.byref(sp), _ptr(d_rows), m, C.byref(p), _ptr(out.transforms),
+                                           _ptr(out.sh_coeffs), _ptr(out.raw_opacities), _stream()))
+    if check:
+        ctx.sync_status()
+    return out
+
+
+class SplatEvaluationRenderer:
+    """training/evaluation/core.rs:343-375 on the GPU: renders splats from a
+    camera with the training rasterizer (so evaluation sees what training
+    optimises) and returns RGB in [0, 1], [H*W*3], quantised to 1/255 as the
+    reference's u8 renderer output is."""
+
+    def __init__(self, render_width: int, render_height: int, raster_cov_blur: float = DEFAULT_RASTER_COV_BLUR,
+                 max_splats: int = 1 << 20, background=(0.0, 0.0, 0.0)):
+        self.width, self.height = int(render_width), int(render_height)
+        self.cov_blur = float(raster_cov_blur)
+        self.background = background
+        self._max = int(max_splats)
+        self._ctx = None
+
+    def _context(self, n):
+        if self._ctx is None or n > self._max:
+            self._max = max(self._max, n)
+            self._ctx = Context(max_splats=self._max, max_pixels=self.width * self.height, cov_blur=self.cov_blur,
+                                background=self.background)
+        return self._ctx
+
+    def render(self, splats, camera: Camera) -> np.ndarray:
+        if not isinstance(splats, DeviceSplats):
+            splats = host_splats_to_device(splats)
+        if camera.width != self.width or camera.height != self.height:
+            raise ValueError("camera size differs from the renderer's")
+        ctx = self._context(splats.num_splats())
+        flat, _, _ = ctx.render_forward(splats, [camera], check=True)
+        rgb = flat.view(self.height, self.width, 4)[..., :3]
+        q = torch.round(torch.clamp(rgb, 0.0, 1.0) * 255.0) / 255.0
+        return q.reshape(-1).cpu().numpy()
+
+
 class Trainer:
     """The device part of WgpuTrainer::train_step (engine/trainer.rs:253-440):
     render all views, 0.8 L1 + 0.2 D-SSIM, backward, densification statistics

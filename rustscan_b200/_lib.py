@@ -110,6 +110,18 @@ class gsr_train_params(C.Structure):
     ]
 
 
+GSR_TOPO_EXISTING, GSR_TOPO_REFINE_EXISTING, GSR_TOPO_REFINE_NEW = 0, 1, 2
+
+
+class gsr_topo_row(C.Structure):
+    _fields_ = [("source", C.c_uint32), ("kind", C.c_int32), ("sample_scalar", C.c_float), ("_pad", C.c_uint32)]
+
+
+class gsr_topo_params(C.Structure):
+    _fields_ = [("has_refine_decay", C.c_int32), ("scale_decay", C.c_float), ("opacity_decay", C.c_float),
+                ("train_t", C.c_float), ("opacity_reset", C.c_int32), ("opacity_reset_cap", C.c_float)]
+
+
 GSR_TUNE_CANDIDATES = 9
 
 
@@ -144,6 +156,7 @@ EXPORTED = [
     "gsr_profile_read",
     "gsr_graph_kernel_count",
     "gsr_autotune",
+    "gsr_topology_apply",
 ]
 
 PROFILE_STAGES = ("project", "depth_sort", "offsets", "emit", "tile_sort", "ranges", "raster_fwd", "visible", "loss",
@@ -190,6 +203,7 @@ def load():
     L.gsr_profile.argtypes = [vp, i32]
     L.gsr_profile_read.argtypes = [vp, C.POINTER(C.c_float), i32, vp]
     L.gsr_graph_kernel_count.argtypes = [vp]
+    L.gsr_topology_apply.argtypes = [vp, C.POINTER(gsr_splats), vp, u32, C.POINTER(gsr_topo_params), vp, vp, vp, vp]
     L.gsr_autotune.argtypes = [C.POINTER(gsr_config), C.POINTER(gsr_splats), C.POINTER(gsr_camera), u32, i32,
                                C.POINTER(gsr_tune_result), vp]
     for name in EXPORTED:

@@ -394,6 +394,7 @@ gsr_status gsr_sync_status(gsr_ctx* c, void* stream, uint64_t* required) {
     snprintf(buf, sizeof(buf), "bounded device wait gave up (site %u)", h.timeout_where);
     return fail(c, GSR_ERR_TIMEOUT, buf);
   }
+  if (h.bad_input) return fail(c, GSR_ERR_INVALID_ARG, "a topology plan row names a source splat out of range");
   if (h.overflow) {
     char buf[128];
     snprintf(buf, sizeof(buf), "intersection capacity %llu exceeded: %llu required",
@@ -716,6 +717,28 @@ gsr_status gsr_profile_read(gsr_ctx* c, float* ms_per_stage, int32_t n_stages, v
 }
 
 int32_t gsr_graph_kernel_count(const gsr_ctx* c) { return c ? c->graph_kernels : 0; }
+
+gsr_status gsr_topology_apply(gsr_ctx* c, const gsr_splats* sp, const gsr_topo_row* rows, uint32_t m,
+                              const gsr_topo_params* params, float* dst_transforms, void* dst_sh,
+                              float* dst_raw_opacity, void* stream) {
+  if (!c) return GSR_ERR_INVALID_ARG;
+  gsr_status rs = check_splats(c, sp);
+  if (rs != GSR_OK) return rs;
+  if (m > 0 && (!rows || !params || !dst_transforms || !dst_sh || !dst_raw_opacity))
+    return fail(c, GSR_ERR_INVALID_ARG, "null topology buffer");
+  if (m == 0) return GSR_OK;
+  static_assert(sizeof(gsr_topo_row) == sizeof(TopoRow), "plan row layout");
+  TopoParams p{};
+  p.has_decay = params->has_refine_decay;
+  p.scale_decay = params->scale_decay;
+  p.opacity_decay = params->opacity_decay;
+  p.train_t = params->train_t;
+  p.opacity_reset = params->opacity_reset;
+  p.reset_cap = params->opacity_reset_cap;
+  GSR_CUDA(c, launch_topology(splats_dev(c, sp), reinterpret_cast<const TopoRow*>(rows), m, p, dst_transforms, dst_sh,
+                              dst_raw_opacity, c->s.status, (cudaStream_t)stream, c->num_sms));
+  return GSR_OK;
+}
 
 gsr_status gsr_autotune(const gsr_config* base, const gsr_splats* sp, const gsr_camera* cams, uint32_t n_views,
                         int32_t reps, gsr_tune_result* out, void* stream) {

@@ -17,7 +17,7 @@ struct DevStatus {
   uint32_t overflow;       // an intersection list did not fit
   uint32_t timeout;        // a bounded wait gave up
   uint32_t timeout_where;  // which wait gave up (kernel id)
-  uint32_t pad;
+  uint32_t bad_input;      // an input index out of range (topology plan)
   unsigned long long required;  // largest intersection count requested
 };
 

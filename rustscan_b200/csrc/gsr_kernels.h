@@ -168,6 +168,16 @@ cudaError_t launch_adam(const AdamArgs& a, const float* g_tr, const float* g_sh,
 cudaError_t launch_densify(const float* v_tr, const float* stats, const float* v_sh, const float* visible, uint32_t n,
                            int degree, int use_visible, float* acc, cudaStream_t st, int num_sms);
 
+// Topology apply: output row i from plan row i (source, kind, sample).
+struct TopoRow {
+  uint32_t source;
+  int32_t kind;
+  float sample;
+  uint32_t pad;
+};
+cudaError_t launch_topology(const SplatsDev& sp, const TopoRow* rows, uint32_t m, const TopoParams& p, float* otr,
+                            void* osh, float* oop, DevStatus* status, cudaStream_t st, int num_sms);
+
 // Loss: per view, l1_w*L1 + ssim_w*(1-SSIM); writes loss[v] and v_pred (RGBA).
 cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const float* pred, const float* target,
                         float l1_w, float ssim_w, float* loss, float* v_pred, float* work, uint64_t work_floats,

@@ -1097,4 +1097,98 @@ GSR_HD void blend_step_grad(F dx, F dy, F ca, F cb, F cc, F r, F gcol, F bcol, F
   g.abs_xy[1] = gabs(g.v_xy[1]);
 }
 
+// ----------------------------------------------------------------------------
+// Topology mutation of one splat row (RustGS/src/training/topology/apply.rs:
+// 29-176): a row copies a source splat, optionally refined as one half of a
+// split (moved by -/+ the rotated, scaled sample offset, its largest axis
+// halved, opacity 1 - sqrt(1 - o)), optionally decayed (scale and opacity
+// shrink with the remaining training fraction) and optionally opacity-reset
+// (capped). Logits go through the numerically stable sigmoid of apply.rs.
+// ----------------------------------------------------------------------------
+enum TopoKind { kTopoExisting = 0, kTopoRefineExisting = 1, kTopoRefineNew = 2 };
+struct TopoParams {
+  int has_decay;
+  float scale_decay, opacity_decay, train_t;
+  int opacity_reset;
+  float reset_cap;
+};
+
+template <class F> GSR_HD F stable_sigmoid(F x) {
+  if (x >= F(0)) {
+    const F e = gexp(-x);
+    return F(1) / (F(1) + e);
+  }
+  const F e = gexp(x);
+  return e / (F(1) + e);
+}
+template <class F> GSR_HD F clamp_to(F x, F lo, F hi) { return gmin(gmax(x, lo), hi); }
+
+// Rotation of v by the quaternion (w, x, y, z), normalised first; a zero
+// quaternion is the identity (apply.rs:97-106).
+template <class F> GSR_HD V3<F> quat_rotate(V4<F> q, V3<F> v) {
+  const F n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+  if (!(n2 > F(0))) return v;
+  const F r = F(1) / gsqrt(n2);
+  const F w = q.x * r, x = q.y * r, y = q.z * r, z = q.w * r;
+  // v + 2w (u x v) + 2 u x (u x v), u = (x, y, z)
+  const F cx = y * v.z - z * v.y, cy = z * v.x - x * v.z, cz = x * v.y - y * v.x;
+  const F dx = y * cz - z * cy, dy = z * cx - x * cz, dz = x * cy - y * cx;
+  V3<F> o;
+  o.x = v.x + F(2) * (w * cx + dx);
+  o.y = v.y + F(2) * (w * cy + dy);
+  o.z = v.z + F(2) * (w * cz + dz);
+  return o;
+}
+
+// One output row from its source row: transforms t[10] (position, quaternion
+// w x y z, log scale) and the opacity logit, in place.
+template <class F> GSR_HD void topo_mutate(F* t, F& logit, int kind, F sample, const TopoParams& p) {
+  if (kind == kTopoRefineExisting || kind == kTopoRefineNew) {
+    V3<F> sc;
+    sc.x = gexp(t[7]);
+    sc.y = gexp(t[8]);
+    sc.z = gexp(t[9]);
+    V3<F> sv;
+    sv.x = sc.x * sample;
+    sv.y = sc.y * sample;
+    sv.z = sc.z * sample;
+    const V3<F> off = quat_rotate(V4<F>{t[3], t[4], t[5], t[6]}, sv);
+    const F sgn = kind == kTopoRefineNew ? F(1) : F(-1);
+    t[0] = t[0] + sgn * off.x;
+    t[1] = t[1] + sgn * off.y;
+    t[2] = t[2] + sgn * off.z;
+    // The largest axis (first on ties) halves (apply.rs:108-118).
+    F r[3] = {sc.x, sc.y, sc.z};
+    int m = 0;
+    for (int a = 1; a < 3; ++a)
+      if (r[a] > r[m]) m = a;
+    r[m] = r[m] * F(0.5);
+    for (int a = 0; a < 3; ++a) t[7 + a] = glog(gmax(r[a], F(1e-6)));
+    // apply.rs:120-124
+    const F lo = F(1.0 / 255.0), hi = F(1) - F(1.0 / 255.0);
+    const F o = clamp_to(stable_sigmoid(logit), lo, hi);
+    const F rf = clamp_to(F(1) - gsqrt(F(1) - o), lo, hi);
+    logit = glog(rf / (F(1) - rf));
+  }
+  if (p.has_decay) {
+    // apply.rs:132-153
+    const F shrink = F(1) - clamp_to(F(p.train_t), F(0), F(1));
+    if (F(p.scale_decay) > F(0)) {
+      const F scaling = gmax(F(1) - F(p.scale_decay) * shrink, F(1e-6));
+      for (int a = 0; a < 3; ++a) t[7 + a] = glog(gmax(gexp(t[7 + a]) * scaling, F(1e-12)));
+    }
+    if (F(p.opacity_decay) > F(0)) {
+      const F o = stable_sigmoid(logit);
+      const F d = clamp_to(o - F(p.opacity_decay) * shrink, F(1e-12), F(1) - F(1e-12));
+      logit = glog(d / (F(1) - d));
+    }
+  }
+  if (p.opacity_reset) {
+    // apply.rs:126-130
+    const F o = clamp_to(stable_sigmoid(logit), F(1e-12), F(1) - F(1e-12));
+    const F r = gmin(o, F(p.reset_cap));
+    logit = glog(r / (F(1) - r));
+  }
+}
+
 }  // namespace gsr

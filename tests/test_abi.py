@@ -51,6 +51,8 @@ def test_struct_layouts_match_header():
         "gsr_train_params": _lib.gsr_train_params,
         "gsr_tune_candidate": _lib.gsr_tune_candidate,
         "gsr_tune_result": _lib.gsr_tune_result,
+        "gsr_topo_row": _lib.gsr_topo_row,
+        "gsr_topo_params": _lib.gsr_topo_params,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():

@@ -258,3 +258,46 @@ def test_reference_cpu_forward_single_splat():
     assert c[0] > 0.2 and abs(c[1] / c[0] - 0.5) < 1e-3 and abs(c[2] / c[0] - 0.25) < 1e-3
     assert col.min() >= 0.0 and col.max() <= 1.0
     assert np.all(dep[0, 0] == np.float32(np.finfo(np.float32).max))
+
+
+def _topo_row_scene(pos, scales, quat, opacity):
+    import numpy as np
+
+    tr = np.array([[*pos, *quat, *np.log(np.asarray(scales, np.float64))]], np.float32)
+    op = np.array([np.log(opacity / (1.0 - opacity))], np.float32)
+    sh = np.zeros((1, 1, 3), np.float32)
+    return tr, sh, op
+
+
+def test_topology_known_answers():
+    """topology/apply.rs tests and topology/tests.rs:1109-1243 restated:
+    the refine offset is the scale rotated by the normalised quaternion (a
+    zero quaternion is the identity), the opacity reset caps 0.8 at 0.01 and
+    leaves 0.005, refine decay at t = 0.5 takes scale 0.1 to 0.09 and
+    opacity 0.5 to 0.45, and a split halves the largest axis and maps the
+    opacity to 1 - sqrt(1 - o)."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    s2 = np.sqrt(0.5)
+    tr, sh, op = _topo_row_scene([0, 0, 0], [2.0, 1e-3, 1e-3], [2 * s2, 0, 0, 2 * s2], 0.5)
+    t, _, _ = O.topology_apply(tr, sh, op, [(0, 2, 1.0)])
+    np.testing.assert_allclose(t[0, :3], [0.0, 2.0, 0.0], atol=2e-3)
+    tr, sh, op = _topo_row_scene([0, 0, 0], [1.0, 2.0, 3.0], [0, 0, 0, 0], 0.5)
+    t, _, o = O.topology_apply(tr, sh, op, [(0, 2, 0.5), (0, 1, 0.5)])
+    np.testing.assert_allclose(t[0, :3], [0.5, 1.0, 1.5], rtol=1e-5)
+    np.testing.assert_allclose(t[1, :3], [-0.5, -1.0, -1.5], rtol=1e-5)
+    np.testing.assert_allclose(np.exp(t[0, 7:10]), [1.0, 2.0, 1.5], rtol=1e-5)  # largest axis halved
+    np.testing.assert_allclose(1 / (1 + np.exp(-o[0])), 1 - np.sqrt(0.5), rtol=1e-5)
+    tr = np.zeros((2, 10), np.float32)
+    tr[:, 3] = 1
+    tr[:, 7:10] = np.log(0.05)
+    op = np.log(np.array([0.8 / 0.2, 0.005 / 0.995], np.float32))
+    _, _, o = O.topology_apply(tr, np.zeros((2, 1, 3), np.float32), op, [(0, 0, 0), (1, 0, 0)], opacity_reset=True)
+    np.testing.assert_allclose(1 / (1 + np.exp(-o)), [0.01, 0.005], atol=1e-6)
+    tr, sh, op = _topo_row_scene([0, 0, 1], [0.1, 0.1, 0.1], [1, 0, 0, 0], 0.5)
+    t, _, o = O.topology_apply(tr, sh, op, [(0, 0, 0)], has_decay=True, scale_decay=0.2, opacity_decay=0.1,
+                               train_t=0.5)
+    np.testing.assert_allclose(np.exp(t[0, 7]), 0.09, atol=1e-6)
+    np.testing.assert_allclose(1 / (1 + np.exp(-o[0])), 0.45, atol=1e-6)

@@ -1,0 +1,102 @@
+"""Scene files (RustGS/src/io/scene_io.rs behaviour): PLY round trips in the
+reference's ASCII layout, binary little-endian input with the other opacity
+and SH layouts, SH degree inference, .splat quantisation and the format
+errors the reference reports."""
+import numpy as np
+import pytest
+
+from rustscan_b200 import scene_io as IO
+from rustscan_b200 import scenes as S
+
+
+def _scene(degree, n=37, seed=3):
+    return S.small_scene(n=n, degree=degree, seed=seed)
+
+
+@pytest.mark.parametrize("degree", [0, 1, 3])
+def test_ply_ascii_round_trip(tmp_path, degree):
+    sc = _scene(degree)
+    p = tmp_path / "s.ply"
+    IO.save_splats_ply(p, sc, IO.SplatMetadata(iterations=12, final_loss=0.25, sh_degree=degree))
+    text = p.read_text().split("\n")
+    assert text[:3] == ["ply", "format ascii 1.0", "comment Generated by RustGS"]
+    assert "comment sh_coeff_layout channel_major" in text and "property float f_rest_44" in text
+    back, md = IO.load_splats_ply(p)
+    assert md.iterations == 12 and md.final_loss == 0.25 and md.sh_degree == degree and md.gaussian_count == sc.n
+    np.testing.assert_array_equal(back.transforms, sc.transforms)
+    np.testing.assert_array_equal(back.sh, sc.sh)
+    np.testing.assert_array_equal(back.raw_opacity, sc.raw_opacity)
+
+
+def _binary_ply(path, sc, interleaved, probability, with_degree_comment):
+    n, K = sc.n, sc.sh.shape[1]
+    rest = sc.sh[:, 1:, :].reshape(n, -1) if interleaved else sc.sh[:, 1:, :].transpose(0, 2, 1).reshape(n, -1)
+    opac = 1.0 / (1.0 + np.exp(-sc.raw_opacity)) if probability else sc.raw_opacity
+    cols = [sc.transforms[:, 0], sc.transforms[:, 1], sc.transforms[:, 2], sc.sh[:, 0, 0], sc.sh[:, 0, 1],
+            sc.sh[:, 0, 2]] + [rest[:, i] for i in range(rest.shape[1])] + [opac, sc.transforms[:, 7],
+                                                                            sc.transforms[:, 8], sc.transforms[:, 9],
+                                                                            sc.transforms[:, 3], sc.transforms[:, 4],
+                                                                            sc.transforms[:, 5], sc.transforms[:, 6]]
+    names = ["x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2"] + [f"f_rest_{i}" for i in range(rest.shape[1])] + [
+        "opacity", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    hdr = ["ply", "format binary_little_endian 1.0"]
+    if with_degree_comment:
+        hdr.append(f"comment SH degree: {sc.sh_degree}")
+    hdr.append("comment opacity_representation " + ("probability" if probability else "raw_logit"))
+    hdr.append("comment sh_coeff_layout " + ("interleaved" if interleaved else "channel_major"))
+    hdr += [f"element vertex {n}"] + [f"property float {c}" for c in names] + ["end_header"]
+    body = np.stack([np.asarray(c, np.float32) for c in cols], axis=1).astype("<f4").tobytes()
+    path.write_bytes(("\n".join(hdr) + "\n").encode() + body)
+
+
+@pytest.mark.parametrize("interleaved", [False, True])
+@pytest.mark.parametrize("probability", [False, True])
+def test_ply_binary_layouts(tmp_path, interleaved, probability):
+    sc = _scene(2)
+    p = tmp_path / "b.ply"
+    _binary_ply(p, sc, interleaved, probability, with_degree_comment=False)
+    back, md = IO.load_splats_ply(p)
+    assert md.sh_degree == 2  # inferred from the 24 f_rest values
+    np.testing.assert_array_equal(back.sh, sc.sh)
+    np.testing.assert_array_equal(back.transforms, sc.transforms)
+    if probability:
+        np.testing.assert_allclose(back.raw_opacity, np.clip(sc.raw_opacity, -13.8, 13.8), rtol=0, atol=2e-4)
+    else:
+        np.testing.assert_array_equal(back.raw_opacity, sc.raw_opacity)
+
+
+def test_splat_round_trip_quantised(tmp_path):
+    sc = _scene(0, n=50)
+    sc.transforms[:, 3:7] /= np.linalg.norm(sc.transforms[:, 3:7], axis=1, keepdims=True)
+    p = tmp_path / "s.splat"
+    IO.save_splats(p, sc)
+    assert p.stat().st_size == 32 * sc.n
+    back, md = IO.load_splats(p)
+    assert md.gaussian_count == sc.n and back.sh_degree == 0
+    np.testing.assert_allclose(back.transforms[:, 0:3], sc.transforms[:, 0:3], rtol=0, atol=0)
+    np.testing.assert_allclose(back.transforms[:, 7:10], sc.transforms[:, 7:10], rtol=0, atol=1e-6)
+    rgb0 = np.clip(sc.sh[:, 0, :] * S.SH_C0 + 0.5, 0, 1)
+    rgb1 = back.sh[:, 0, :] * S.SH_C0 + 0.5
+    assert np.abs(rgb1 - rgb0).max() <= 0.5 / 255 + 1e-6
+    q0 = sc.transforms[:, 3:7]
+    q1 = back.transforms[:, 3:7]
+    assert np.abs(np.abs((q0 * q1).sum(1)) - 1).max() < 2e-2
+
+
+def test_format_errors(tmp_path):
+    with pytest.raises(IO.SceneIoError, match="unsupported splat output extension"):
+        IO.save_splats(tmp_path / "x.obj", _scene(0))
+    with pytest.raises(IO.SceneIoError, match="missing splat output extension"):
+        IO.load_splats(tmp_path / "noext")
+    bad = tmp_path / "bad.splat"
+    bad.write_bytes(b"\0" * 33)
+    with pytest.raises(IO.SceneIoError, match="multiple of 32"):
+        IO.load_splats(bad)
+    nomagic = tmp_path / "n.ply"
+    nomagic.write_bytes(b"plx\n")
+    with pytest.raises(IO.SceneIoError, match="magic"):
+        IO.load_splats(nomagic)
+    missing = tmp_path / "m.ply"
+    missing.write_bytes(b"ply\nformat ascii 1.0\nelement vertex 0\nproperty float x\nend_header\n")
+    with pytest.raises(IO.SceneIoError, match="missing required PLY property y"):
+        IO.load_splats(missing)
