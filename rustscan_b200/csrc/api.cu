@@ -153,7 +153,8 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.isect_key_raw, nv * I) && dalloc(c, &b.isect_val_raw, nv * I) &&
             dalloc(c, &b.ranges, nv * 2 * T) && dalloc(c, &b.tfinal, nv * P) && dalloc(c, &b.last, nv * P) &&
             dalloc(c, &b.ncontrib, nv * P) && dalloc(c, &b.nvisit, nv * P) && dalloc(c, &b.visible_c, nv * V) &&
-            dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4);
+            dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4) &&
+            dalloc(c, &b.tile_hist, nv * T);
   if (ok && cfg.deterministic)
     ok = dalloc(c, &b.sgrad_part, nv * I * 12) && dalloc(c, &b.inv_perm, nv * I);
   else {
@@ -290,13 +291,23 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   GSR_CUDA(c, launch_count(vs, b, c->s, st));
   GSR_CUDA(c, launch_offsets(vs, b, c->s, st));
   prof_mark(c, kStEmit, st);
-  GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));
+  // Up to kHistMaxTiles tiles a view, emission also counts intersections
+  // per tile: the tile ranges and the tile sort's digit histograms follow
+  // from those counts (no histogram pass, no ranges pass).
+  const bool tile_counts = vs.max_tiles <= kHistMaxTiles;
+  if (tile_counts) {
+    GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, st));
+    GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, st));
+  } else {
+    GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));
+  }
   prof_mark(c, kStTileSort, st);
   GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, b.isect_val_raw, b.isect_key, b.isect_val, b.key_tmp, b.val_tmp,
-                               b.Icap, n_views, b.vcount + 1, 4, 0, b.Icap, bits_for(vs.max_tiles), c->s, st));
+                               b.Icap, n_views, b.vcount + 1, 4, 0, b.Icap, bits_for(vs.max_tiles), c->s, st,
+                               tile_counts));
   if (c->cfg.deterministic) GSR_CUDA(c, launch_remap(vs, b, c->s, st));
   prof_mark(c, kStRanges, st);
-  GSR_CUDA(c, launch_ranges(vs, b, c->s, st));
+  if (!tile_counts) GSR_CUDA(c, launch_ranges(vs, b, c->s, st));
   prof_mark(c, kStRasterFwd, st);
   GSR_CUDA(c, launch_raster_fwd(vs, b, c->cfg.background, out_rgba, c->s, st));
   prof_mark(c, kStVisible, st);

@@ -28,6 +28,7 @@ struct FwdBufs {
   uint32_t* isect_key_raw; // [I] emission order
   uint32_t* isect_val_raw;
   uint32_t* ranges;        // [2T]
+  uint32_t* tile_hist;     // [T] intersections per tile (counted during emission)
   float* tfinal;           // [P] final transmittance
   uint32_t* last;          // [P] last contributor list index + 1
   uint32_t* ncontrib;      // [P]
@@ -85,7 +86,8 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
                              uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
-                             uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st);
+                             uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st,
+                             bool hist_ready = false);
 
 // Inclusive scan of n_host values (prefix sum primitive).
 cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_host, const Scratch& s,
@@ -102,6 +104,13 @@ cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cuda
 // Per-view tile counts of the compact records (count[c], gid order).
 cudaError_t launch_count(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
+// Emission that also counts the emitted intersections per tile (tile_hist),
+// then, from those counts, the tile ranges and the tile sort's per-pass digit
+// histograms (Scratch::hist), replacing the sort's histogram pass and the
+// ranges kernel. For views of at most kHistMaxTiles tiles.
+constexpr uint32_t kHistMaxTiles = 8192;
+cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_remap(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_ranges(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 

@@ -40,9 +40,10 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 // Gaussian's scanned offset; then replace the record's tile box with the
 // footprint half-widths the rasterizer culls warp blocks with (negative: no
 // box, never cull).
-template <bool EMIT>
+template <bool EMIT, bool HIST = false>
 __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, FwdBufs b, int det) {
   __shared__ WalkWarp s_w[kWalkWarps];
+  extern __shared__ uint32_t s_th[];  // HIST: per-tile counts of this block's emitted intersections
   const uint32_t v = blockIdx.y;
   const uint32_t V = b.vcount[v * 4 + 0];
   const ViewDesc& vd = vs.views[v];
@@ -58,6 +59,11 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
   const uint64_t cap = b.Icap;
   const uint32_t lane = threadIdx.x & 31u;
   WalkWarp& S = s_w[threadIdx.x >> 5];
+  const uint32_t T = vd.tiles_x * vd.tiles_y;
+  if (HIST) {
+    for (uint32_t t = threadIdx.x; t < T; t += kWalkThreads) s_th[t] = 0u;
+    __syncthreads();
+  }
   const uint32_t stride = gridDim.x * kWalkWarps * 32u;
   for (uint32_t base = (blockIdx.x * kWalkWarps + (threadIdx.x >> 5)) * 32u; base < V; base += stride) {
     const uint32_t r = base + lane;
@@ -138,6 +144,7 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
         const uint32_t before = pm & ((1u << lane) - 1u) & ~((1u << first) - 1u);
         const uint64_t o = (uint64_t)S.off[owner] + S.run[owner] + (uint32_t)__popc(before);
         if (o < cap) {
+          if (HIST) atomicAdd(&s_th[tx + ty * vd.tiles_x], 1u);
           keys[o] = tx + ty * vd.tiles_x;
           if (det) {
             vals[o] = (uint32_t)o;
@@ -166,6 +173,57 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
         rw->w = ry;
       }
     }
+  }
+  if (HIST) {
+    __syncthreads();
+    uint32_t* th = slice(b.tile_hist, b.Tcap, v);
+    for (uint32_t t = threadIdx.x; t < T; t += kWalkThreads)
+      if (s_th[t]) atomicAdd(th + t, s_th[t]);
+  }
+}
+
+// From the per-tile counts of one view: the tile ranges
+// (get_tile_offsets.wgsl:11-30 — [start, end) per tile, 0,0 when empty) and
+// the digit histograms of the tile sort's two passes (low and high byte of
+// the tile id), in the sort's histogram layout.
+constexpr int kHistThreads = 1024;
+__global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist) {
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_h[2][256];
+  const uint32_t v = blockIdx.x;
+  const ViewDesc& vd = vs.views[v];
+  const uint32_t T = vd.tiles_x * vd.tiles_y;
+  const uint32_t* th = slice(b.tile_hist, b.Tcap, v);
+  uint32_t* ranges = slice(b.ranges, 2 * b.Tcap, v);
+  for (int i = threadIdx.x; i < 512; i += kHistThreads) (&s_h[0][0])[i] = 0u;
+  constexpr uint32_t kPer = kHistMaxTiles / kHistThreads;
+  const uint32_t t0 = threadIdx.x * kPer;
+  uint32_t loc[kPer];
+  uint32_t sum = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < kPer; ++i) {
+    loc[i] = t0 + i < T ? th[t0 + i] : 0u;
+    sum += loc[i];
+  }
+  uint32_t all;
+  uint32_t run = block_exclusive_scan(sum, s_scan, &all);  // its barriers also order the zeroing above
+#pragma unroll
+  for (uint32_t i = 0; i < kPer; ++i) {
+    const uint32_t t = t0 + i;
+    if (t < T) {
+      ranges[2 * t] = loc[i] ? run : 0u;
+      ranges[2 * t + 1] = loc[i] ? run + loc[i] : 0u;
+      if (loc[i]) {
+        atomicAdd(&s_h[0][t & 255u], loc[i]);
+        atomicAdd(&s_h[1][(t >> 8) & 255u], loc[i]);
+      }
+    }
+    run += loc[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 1024; i += kHistThreads) {
+    const int p = i >> 8;
+    hist[(size_t)v * 1024 + i] = p < 2 ? s_h[p][i & 255] : 0u;
   }
 }
 
@@ -267,6 +325,21 @@ cudaError_t launch_count(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaSt
 
 cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st) {
   tile_walk_kernel<true><<<grid_for(vs, s.num_sms), kWalkThreads, 0, st>>>(vs, b, deterministic);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st) {
+  if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(b.tile_hist, 0, sizeof(uint32_t) * b.Tcap * vs.n_views, st);
+  if (e != cudaSuccess) return e;
+  const size_t smem = sizeof(uint32_t) * vs.max_tiles;
+  tile_walk_kernel<true, true><<<grid_for(vs, s.num_sms), kWalkThreads, smem, st>>>(vs, b, deterministic);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
+  if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
+  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist);
   return cudaGetLastError();
 }
 

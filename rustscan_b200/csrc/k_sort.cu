@@ -266,16 +266,16 @@ int persistent_blocks(int num_sms, uint32_t segments, int per_sm) {
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride, uint32_t segments,
                              const uint32_t* counts, uint32_t count_stride, uint32_t n_host, uint64_t cap_per_segment,
-                             int bits, const Scratch& s, cudaStream_t st) {
+                             int bits, const Scratch& s, cudaStream_t st, bool hist_ready) {
   if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
   int passes = (bits + 7) / 8;
   if (passes < 1) passes = 1;
   if (passes > 4) passes = 4;
   const uint32_t parts_cap = (uint32_t)((cap_per_segment + kSortTile - 1) / kSortTile);
   if ((uint64_t)parts_cap * 256 * segments > s.lb_states_words) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 1024 * segments, st);
-  if (e != cudaSuccess) return e;
-  {
+  if (!hist_ready) {
+    cudaError_t e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 1024 * segments, st);
+    if (e != cudaSuccess) return e;
     dim3 grid(persistent_blocks(s.num_sms, segments, 4), segments);
     sort_hist_kernel<<<grid, 256, 0, st>>>(keys_in, seg_stride, counts, count_stride, n_host, cap_per_segment, passes,
                                            s.hist);
