@@ -326,6 +326,12 @@ GSR_API gsr_status gsr_autotune(const gsr_config* base, const gsr_splats* splats
 enum { GSR_PROFILE_STAGES = 13 };
 GSR_API gsr_status gsr_profile(gsr_ctx* ctx, int32_t enable);
 GSR_API gsr_status gsr_profile_read(gsr_ctx* ctx, float* ms_per_stage, int32_t n_stages, void* stream);
+/* Self-test of the bounded device waits (no counterpart in the reference):
+ * runs one look-back whose predecessor never publishes, which must give up
+ * after max_polls polls (1..2^22). Returns GSR_ERR_TIMEOUT when the wait gave
+ * up as it should (the context stays usable), GSR_OK if it did not.
+ * Synchronises the stream. */
+GSR_API gsr_status gsr_selftest_wait_timeout(gsr_ctx* ctx, uint32_t max_polls, void* stream);
 /* Kernel nodes in the captured training-step graph (0 before a capture). */
 GSR_API int32_t gsr_graph_kernel_count(const gsr_ctx* ctx);
 

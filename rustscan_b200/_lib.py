@@ -157,6 +157,7 @@ EXPORTED = [
     "gsr_graph_kernel_count",
     "gsr_autotune",
     "gsr_topology_apply",
+    "gsr_selftest_wait_timeout",
 ]
 
 PROFILE_STAGES = ("project", "depth_sort", "offsets", "emit", "tile_sort", "ranges", "raster_fwd", "visible", "loss",
@@ -204,6 +205,7 @@ def load():
     L.gsr_profile_read.argtypes = [vp, C.POINTER(C.c_float), i32, vp]
     L.gsr_graph_kernel_count.argtypes = [vp]
     L.gsr_topology_apply.argtypes = [vp, C.POINTER(gsr_splats), vp, u32, C.POINTER(gsr_topo_params), vp, vp, vp, vp]
+    L.gsr_selftest_wait_timeout.argtypes = [vp, u32, vp]
     L.gsr_autotune.argtypes = [C.POINTER(gsr_config), C.POINTER(gsr_splats), C.POINTER(gsr_camera), u32, i32,
                                C.POINTER(gsr_tune_result), vp]
     for name in EXPORTED:

@@ -729,6 +729,17 @@ gsr_status gsr_profile_read(gsr_ctx* c, float* ms_per_stage, int32_t n_stages, v
 
 int32_t gsr_graph_kernel_count(const gsr_ctx* c) { return c ? c->graph_kernels : 0; }
 
+gsr_status gsr_selftest_wait_timeout(gsr_ctx* c, uint32_t max_polls, void* stream) {
+  if (!c) return GSR_ERR_INVALID_ARG;
+  if (max_polls < 1 || max_polls > kMaxPolls) return fail(c, GSR_ERR_INVALID_ARG, "max_polls outside 1..2^22");
+  if (c->s.lb_states_words < 2) return fail(c, GSR_ERR_INVALID_ARG, "no look-back scratch");
+  // The probe overwrites look-back states 0 and 1; every look-back launch
+  // tags its states with a fresh epoch, so later launches are unaffected.
+  GSR_CUDA(c, launch_lookback_timeout_probe(c->s.lb_states, c->s.status, max_polls, c->b.vcount + 3,
+                                            (cudaStream_t)stream));
+  return gsr_sync_status(c, stream, nullptr);
+}
+
 gsr_status gsr_topology_apply(gsr_ctx* c, const gsr_splats* sp, const gsr_topo_row* rows, uint32_t m,
                               const gsr_topo_params* params, float* dst_transforms, void* dst_sh,
                               float* dst_raw_opacity, void* stream) {

@@ -21,7 +21,7 @@ struct DevStatus {
   unsigned long long required;  // largest intersection count requested
 };
 
-enum : uint32_t { kWaitCompact = 1, kWaitScan = 2, kWaitSort = 3 };
+enum : uint32_t { kWaitCompact = 1, kWaitScan = 2, kWaitSort = 3, kWaitSelfTest = 4 };
 
 // Per-view camera and layout, in device memory.
 struct ViewDesc {
@@ -91,7 +91,8 @@ __device__ __forceinline__ void st_volatile64(unsigned long long* p, unsigned lo
 // Publishes `agg` for partition `part` of a chain whose states are
 // states[part * stride] and returns the exclusive prefix of the partition.
 __device__ __forceinline__ uint32_t lookback(unsigned long long* states, uint32_t stride, uint32_t part, uint32_t agg,
-                                             uint32_t epoch, DevStatus* status, uint32_t where) {
+                                             uint32_t epoch, DevStatus* status, uint32_t where,
+                                             uint32_t max_polls = kMaxPolls) {
   const unsigned long long tag = (unsigned long long)(epoch & 0x3fffffffu) << 34;
   if (part == 0) {
     st_volatile64(states, tag | kFlagPre | agg);
@@ -124,7 +125,7 @@ __device__ __forceinline__ uint32_t lookback(unsigned long long* states, uint32_
     j -= used;
     if (!done && used < kLookbackWindow && j >= 0) {
       // Stopped at an unpublished predecessor.
-      if (++polls > kMaxPolls) {
+      if (++polls > max_polls) {
         report_timeout(status, where);
         break;
       }

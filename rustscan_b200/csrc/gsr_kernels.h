@@ -89,6 +89,11 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st,
                              bool hist_ready = false);
 
+// Bounded-wait self-test: a look-back whose predecessor never publishes
+// (look-back states 0 and 1 are overwritten); gives up after max_polls.
+cudaError_t launch_lookback_timeout_probe(unsigned long long* states, DevStatus* status, uint32_t max_polls,
+                                          uint32_t* out, cudaStream_t st);
+
 // Inclusive scan of n_host values (prefix sum primitive).
 cudaError_t inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n_host, const Scratch& s,
                                cudaStream_t st);

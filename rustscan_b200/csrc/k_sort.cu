@@ -381,3 +381,26 @@ cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cuda
 }
 
 }  // namespace gsr
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded wait: one thread plays partition 1 of a look-back
+// whose partition 0 never publishes (its state word carries another epoch),
+// so the wait must give up after max_polls polls, flag the status and return.
+// ---------------------------------------------------------------------------
+namespace gsr {
+namespace {
+__global__ void lookback_timeout_probe_kernel(unsigned long long* states, DevStatus* status, uint32_t max_polls,
+                                              uint32_t* out) {
+  if (threadIdx.x == 0) {
+    states[0] = 0ull;  // epoch 0: never the probe's epoch below
+    *out = lookback(states, 1, 1, 7u, 0x3fffffffu, status, kWaitSelfTest, max_polls);
+  }
+}
+}  // namespace
+
+cudaError_t launch_lookback_timeout_probe(unsigned long long* states, DevStatus* status, uint32_t max_polls,
+                                          uint32_t* out, cudaStream_t st) {
+  lookback_timeout_probe_kernel<<<1, 32, 0, st>>>(states, status, max_polls, out);
+  return cudaGetLastError();
+}
+}  // namespace gsr

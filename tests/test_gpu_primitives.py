@@ -1,6 +1,7 @@
 """Scan and sort primitives through the C ABI against the reference's known
 answers (gpu_primitives/{prefix_sum,radix_sort}/tests.rs) and numpy."""
 import json
+import time
 import os
 
 import numpy as np
@@ -72,3 +73,26 @@ def test_sort_repeat_is_deterministic(ctx):
     a = _np(ctx.radix_sort_by_key_u32(_t(keys), _t(np.arange(keys.size)))[1])
     b = _np(ctx.radix_sort_by_key_u32(_t(keys), _t(np.arange(keys.size)))[1])
     np.testing.assert_array_equal(a, b)
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(ctx):
+    """A look-back whose predecessor never publishes (a flag nothing sets)
+    gives up after its poll limit and reports GSR_ERR_TIMEOUT with the wait
+    site; no fault, no hang, and the context keeps working afterwards."""
+    import ctypes as C
+
+    import torch
+
+    t0 = time.perf_counter()
+    st = ctx._lib.gsr_selftest_wait_timeout(ctx._h, 1 << 14, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    dt = time.perf_counter() - t0
+    assert st == 5, st
+    assert b"bounded device wait gave up (site 4)" in ctx._lib.gsr_last_error(ctx._h)
+    assert dt < 10.0
+    # A scan (look-back) right after works and is exact.
+    x = np.arange(5000, dtype=np.uint32) % 7
+    out = ctx.prefix_sum_u32(_t(x))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), np.cumsum(x, dtype=np.uint32))
+    ctx.sync_status()
+
