@@ -144,10 +144,11 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
-def make_context(n, views, sh_dtype="f32"):
+def make_context(n, views, sh_dtype="f32", tile=(16, 16), batch=0):
     from rustscan_b200 import Context
 
-    return Context(max_splats=n, max_views=views, max_pixels=1280 * 720, max_isects=24 << 20, sh_dtype=sh_dtype)
+    return Context(max_splats=n, max_views=views, max_pixels=1280 * 720, max_isects=24 << 20, sh_dtype=sh_dtype,
+                   tile=tile, batch=batch)
 
 
 def fit_capacity(ctx, splats, cams):
@@ -313,14 +314,21 @@ def main():
     nv = len(cams)
     H, W = cams[0].height, cams[0].width
 
+    # Tile shape and raster batch from the autotuner (untimed), as a user
+    # would pick them for this scene and view mix.
+    from rustscan_b200 import autotune
+
+    splats = host_splats_to_device(sc)
+    tuned = autotune(splats, cams, reps=2, max_pixels=W * H, max_isects=24 << 20)
+    tile, batch = tuned["tile"], tuned["batch"]
+
     # Targets: renders of the hidden ground-truth set.
-    ctx = make_context(args.n, nv)
+    ctx = make_context(args.n, nv, tile=tile, batch=batch)
     gts = host_splats_to_device(S.Scene(gt_tr, gt_sh, gt_op, 3, cams))
     fit_capacity(ctx, gts, cams)
     flat, _, _ = ctx.render_forward(gts, cams)
     targets = flat.view(nv, H, W, 4)[..., :3].contiguous()
     del gts
-    splats = host_splats_to_device(sc)
     fit_capacity(ctx, splats, cams)
     counts = [ctx.export(v, "counts") for v in range(nv)]
     V = [int(c[0]) for c in counts]
@@ -378,7 +386,7 @@ def main():
     # ---- plain single-view path (one view per call, FP32, no graph) ------------
     plain = None
     if not args.no_plain:
-        ctx1 = make_context(args.n, 1)
+        ctx1 = make_context(args.n, 1, tile=tile, batch=batch)
         fit_capacity(ctx1, splats, [cams[0]])
         tr1 = Trainer(ctx1, splats, LearningRates(), use_graph=False)
 
@@ -415,8 +423,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; see rustscan_b200/scenes.py)",
             "config": {"workload": WORKLOAD, "n_gaussians": args.n, "views_per_step": nv, "resolution": f"{W}x{H}",
-                       "sh_degree": 3, "sh_storage": "f32", "tile": "16x16", "loss": "0.8 L1 + 0.2 D-SSIM",
-                       "optimizer": "fused Adam (lr_pos 1.6e-4)", "graph": True,
+                       "sh_degree": 3, "sh_storage": "f32", "tile": f"{tile[0]}x{tile[1]}",
+                       "raster_batch": batch, "tile_and_batch": "autotuner (gsr_autotune)",
+                       "loss": "0.8 L1 + 0.2 D-SSIM", "optimizer": "Adam (lr_pos 1.6e-4)", "graph": True,
                        "l2": "inputs larger than L2 (params 236 MB + 8 views of state per step)",
                        "visible_per_view": V, "intersections_per_view": I, "parallelism": "replicas" if world > 1 else "1 GPU"},
             "plain_single_view_ms_per_view": plain,
