@@ -154,7 +154,7 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.ranges, nv * 2 * T) && dalloc(c, &b.tfinal, nv * P) && dalloc(c, &b.last, nv * P) &&
             dalloc(c, &b.ncontrib, nv * P) && dalloc(c, &b.nvisit, nv * P) && dalloc(c, &b.visible_c, nv * V) &&
             dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4) &&
-            dalloc(c, &b.tile_hist, nv * T);
+            dalloc(c, &b.tile_hist, nv * T) && dalloc(c, &b.hitw, nv * I);
   if (ok && cfg.deterministic)
     ok = dalloc(c, &b.sgrad_part, nv * I * 12) && dalloc(c, &b.inv_perm, nv * I);
   else {

@@ -34,6 +34,7 @@ struct FwdBufs {
   uint32_t* ncontrib;      // [P]
   uint32_t* nvisit;        // [P]
   uint8_t* visible_c;      // [V]
+  uint8_t* hitw;           // [I] per list entry: forward warp blocks with a pixel that took it
   float4* sgrad;           // [V][3] screen-space gradient sums (12 floats)
   float4* pair;            // [views][6][Vcap]: six float4 planes of projection adjoint records
   float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)

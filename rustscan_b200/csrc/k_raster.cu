@@ -16,7 +16,10 @@
 // alpha >= 1/255 test (see kRejectMargin).
 //
 // The forward records per pixel the final transmittance and the list index
-// of the last contributor. The backward walks the same per-warp lists from
+// of the last contributor, and per list entry a bit for each warp block in
+// which some pixel took the Gaussian. The backward walks, per warp, only the
+// entries whose forward bit covers its block (its contributor decisions
+// repeat the forward's, so no other entry can contribute there), from
 // the tile's largest last index down, recovers the transmittance before each
 // contributor by division (T_i = T_{i+1} / (1 - alpha_i)), keeps the colour
 // accumulated behind it, and forms per-pixel gradients (blend_step_grad).
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   __shared__ float4 s_c[BATCH];  // max(r,0), max(g,0), max(b,0), -
   __shared__ uint32_t s_cidx[BATCH];
   __shared__ uint8_t s_mask[BATCH];
-  __shared__ uint8_t s_hit[BATCH];
+  __shared__ uint8_t s_hit[NW][BATCH];  // warp w took entry j
   __shared__ uint16_t s_list[NW][BATCH];
   const uint32_t item = blockIdx.x;
   const uint32_t v = find_view(a.vs, item);
@@ -183,6 +186,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   const uint32_t* vals = slice(a.b.isect_val, a.b.Icap, v);
   const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
   uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
+  uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
   const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
   // Pixel q = 2k + h sits at row pyb + 4q and is half h of pair k.
   float2 T[NP], C0[NP], C1[NP], C2[NP], npcy[NP];
@@ -214,7 +218,8 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
       s_b[j] = B;
       s_c[j] = Cc;
       s_cidx[j] = c;
-      s_hit[j] = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) s_hit[w][j] = 0;
     }
     __syncthreads();
     if (!__all_sync(0xffffffffu, all_done)) {
@@ -249,7 +254,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
           C1[k] = fma2(f2(Cc.y), w, C1[k]);
           C2[k] = fma2(f2(Cc.z), w, C2[k]);
           T[k] = mul2(T[k], add2(f2(1.f), neg2(am)));
-          s_hit[j] = 1;
+          s_hit[warp][j] = 1;
           if (c0) {
             last[2 * k] = b0 + j + 1;
             ++nc[2 * k];
@@ -274,8 +279,13 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
       }
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += NT)
-      if (s_hit[j]) vis[s_cidx[j]] = 1;
+    for (uint32_t j = threadIdx.x; j < nb; j += NT) {
+      uint32_t bits = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) bits |= (uint32_t)s_hit[w][j] << w;
+      hitw[b0 + j] = (uint8_t)bits;
+      if (bits) vis[s_cidx[j]] = 1;
+    }
     if (__syncthreads_and(all_done)) break;
   }
   float4* out = reinterpret_cast<float4*>(a.out_rgba) + vd.pix_base;
@@ -446,6 +456,23 @@ __device__ __forceinline__ uint32_t bwd_pair_step(BwdPair& p, uint32_t s, float 
   return (gm0 ? 1u : 0u) | (gm1 ? 2u : 0u);
 }
 
+// Maps the forward's per-entry warp-block bits (blocks of kFwdPPL pixels
+// per lane) onto the warp blocks of a backward with PB pixels per lane: a
+// backward block is the union of the forward blocks of its column span and
+// rows.
+template <int TW, int TH, int PB>
+__device__ __forceinline__ uint32_t hit_bits_for(uint32_t f) {
+  constexpr int PF = kFwdPPL;
+  static_assert(PB % PF == 0, "backward warp blocks are unions of forward ones");
+  constexpr int NWF = TW * TH / PF / 32;
+  constexpr int KX = TW / 8;
+  if (PB == PF) return f;
+  uint32_t m = 0;
+#pragma unroll
+  for (int fw = 0; fw < NWF; ++fw) m |= ((f >> fw) & 1u) << ((fw % KX) + ((fw / KX) * PF / PB) * KX);
+  return m;
+}
+
 template <int TW, int TH, int PPL, int BATCH>
 __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) {
   static_assert(PPL % 2 == 0, "pixels per lane come in pairs");
@@ -474,6 +501,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   const uint32_t s0 = ranges[2 * t];
   const uint32_t* vals = slice(a.b.isect_val, a.b.Icap, v);
   const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
+  const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
   float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
   float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
   const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
@@ -495,13 +523,19 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     const uint32_t nb = be - bs;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < nb; j += NT) {
-      const uint32_t c = vals[bs + j];
-      float4 A, B, Cc;
-      s_mask[j] = (uint8_t)stage_one<TW, PPL, NW, false>(rec, c, tx0, ty0, A, B, Cc);
-      s_a[j] = A;
-      s_b[j] = B;
-      s_c[j] = Cc;
-      s_cidx[j] = c;
+      // Only the warp blocks that took the entry in the forward can take
+      // it here; an entry no block took is not staged at all.
+      const uint32_t hm = hit_bits_for<TW, TH, PPL>(hitw[bs + j]);
+      s_mask[j] = (uint8_t)hm;
+      if (hm) {
+        const uint32_t c = vals[bs + j];
+        float4 A, B, Cc;
+        (void)stage_one<TW, PPL, NW, false>(rec, c, tx0, ty0, A, B, Cc);
+        s_a[j] = A;
+        s_b[j] = B;
+        s_c[j] = Cc;
+        s_cidx[j] = c;
+      }
     }
     {
       float4* z = &s_part[0][0][0];
