@@ -191,6 +191,9 @@ GSR_API gsr_status gsr_render_backward(gsr_ctx* ctx, const gsr_splats* splats, c
  *  9 per-Gaussian screen-space gradient sums of the last backward (f32 x 12V)
  * 10 per-pixel list entries evaluated (u32 x H*W)
  * 11 per-Gaussian tile counts in compact order (u32 x V)
+ * 12 per-intersection 8x8 pixel blocks of its tile (bit x + (y * tile_w / 8),
+ *    blocks row-major) holding a pixel that took the Gaussian (u8 x I; defined
+ *    for entries before the tile's largest last-contributor index)
  * `bytes` is the destination size; the call fails if it is too small. */
 GSR_API gsr_status gsr_export(gsr_ctx* ctx, uint32_t view, int32_t what, void* dst, uint64_t bytes, void* stream);
 

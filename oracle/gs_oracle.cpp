@@ -94,6 +94,9 @@ template <class F> struct FwdState {
   std::vector<uint32_t> ncontrib;  // number of contributors
   std::vector<uint32_t> nvisit;    // list entries evaluated before termination
   std::vector<F> visible;          // [n]
+  // per intersection: bit (lx/8) + (ly/8)*(tile_w/8) for each 8x8 pixel block
+  // of the tile holding a pixel that took the Gaussian (test inspection)
+  std::vector<uint32_t> hit_blocks;
 };
 
 // ---------------------------------------------------------------------------
@@ -202,6 +205,7 @@ template <class F> void forward(FwdState<F>& st) {
   st.last.assign((size_t)W * H, 0);
   st.ncontrib.assign((size_t)W * H, 0);
   st.nvisit.assign((size_t)W * H, 0);
+  st.hit_blocks.assign(I, 0);
   std::vector<uint8_t> vis_c(V, 0);
 #pragma omp parallel for schedule(dynamic, 4)
   for (long tile = 0; tile < (long)T; ++tile) {
@@ -228,6 +232,7 @@ template <class F> void forward(FwdState<F>& st) {
           C[2] = blend_accum(C[2], st.rgb[c].z, vis);
           Tr = Tr * (F(1) - alpha);
           vis_c[c] = 1;  // benign race: every writer stores 1
+          st.hit_blocks[s] |= 1u << ((lx / 8) + (ly / 8) * ((st.ts.tw + 7) / 8));  // entry s belongs to this tile only
           last = s + 1;
           ++nc;
           if (Tr < F(1e-4)) break;
@@ -663,6 +668,9 @@ ORC_EXPORT float orc_logf(float x) { return portable_logf(x); }
     std::copy(st.ncontrib.begin(), st.ncontrib.end(), nc);                                                        \
     std::copy(st.nvisit.begin(), st.nvisit.end(), nv);                                                            \
     std::copy(st.visible.begin(), st.visible.end(), visible);                                                     \
+  }                                                                                                               \
+  ORC_EXPORT void orc_hit_blocks_##SUF(const orc_fwd_##SUF* h, uint32_t* bits) {                                 \
+    std::copy(h->st.hit_blocks.begin(), h->st.hit_blocks.end(), bits);                                            \
   }                                                                                                               \
   /* backward: mode 0 exact, 1 reference semantics (reverse walk), 2 literal WGSL walk */                         \
   ORC_EXPORT void orc_backward_##SUF(const orc_fwd_##SUF* h, const F* v_rgba, int mode, F* v_tr, F* v_sh, F* v_op, \

@@ -49,6 +49,7 @@ def lib():
             getattr(L, f"orc_visible_{suf}").argtypes = [C.c_void_p, i32p, u32p, fp, fp, u32p]
             getattr(L, f"orc_order_{suf}").argtypes = [C.c_void_p, i32p]
             getattr(L, f"orc_isects_{suf}").argtypes = [C.c_void_p, u32p, u32p, u32p]
+            getattr(L, f"orc_hit_blocks_{suf}").argtypes = [C.c_void_p, u32p]
             getattr(L, f"orc_pixels_{suf}").argtypes = [C.c_void_p, fp, fp, u32p, u32p, u32p, fp]
             getattr(L, f"orc_backward_{suf}").argtypes = [C.c_void_p, fp, C.c_int, fp, fp, fp, fp, fp]
             lf = getattr(L, f"orc_loss_{suf}")
@@ -141,6 +142,13 @@ class Forward:
         self.visible = np.zeros(self.n, dt)
         getattr(L, f"orc_pixels_{self.suf}")(self._h, _p(self.image, fp), _p(self.tfinal, fp), _p(self.last, u32p),
                                               _p(self.ncontrib, u32p), _p(self.nvisit, u32p), _p(self.visible, fp))
+
+    def hit_blocks(self):
+        """Per intersection: bits of the tile's 8x8 pixel blocks (x fastest)
+        holding a pixel that took the Gaussian."""
+        out = np.zeros(max(self.num_intersections, 1), np.uint32)
+        getattr(lib(), f"orc_hit_blocks_{self.suf}")(self._h, _p(out, u32p))
+        return out[:self.num_intersections]
 
     def backward(self, v_rgba, mode=0):
         """mode 0: exact adjoint; 1: reference semantics, reverse walk; 2: literal WGSL walk."""

@@ -31,7 +31,7 @@ from .scenes import Camera, Scene  # noqa: F401  (re-exported)
 DEFAULT_RASTER_COV_BLUR = 0.3  # RustGS/src/training/config.rs:7
 
 EXPORT = dict(counts=0, gids=1, depth_order=2, isect_tiles=3, isect_vals=4, tile_ranges=5, tfinal=6, last=7,
-              ncontrib=8, splat_grads=9, nvisit=10, tile_counts=11)
+              ncontrib=8, splat_grads=9, nvisit=10, tile_counts=11, hit_blocks=12)
 
 
 def _require_cuda():
@@ -259,7 +259,7 @@ class Context:
         ty = math.ceil(cam.height / self.cfg.tile_h)
         shapes = {0: (2, np.uint32), 1: (V, np.uint32), 2: (V, np.uint32), 3: (I, np.uint32), 4: (I, np.uint32),
                   5: (2 * tx * ty, np.uint32), 6: (P, np.float32), 7: (P, np.uint32), 8: (P, np.uint32),
-                  9: (12 * V, np.float32), 10: (P, np.uint32), 11: (V, np.uint32)}
+                  9: (12 * V, np.float32), 10: (P, np.uint32), 11: (V, np.uint32), 12: (I, np.uint8)}
         if code == 0:
             return cnt
         n, dt = shapes[code]

@@ -519,6 +519,7 @@ gsr_status gsr_export(gsr_ctx* c, uint32_t view, int32_t what, void* dst, uint64
     case 9: src = slice(b.sgrad, b.Vcap * 3, view); need = 48 * V; break;
     case 10: src = slice(b.nvisit, b.Pcap, view); need = 4 * P; break;
     case 11: src = slice(b.count, b.Vcap, view); need = 4 * V; break;
+    case 12: src = slice(b.hitw, b.Icap, view); need = I; break;
     default: return fail(c, GSR_ERR_INVALID_ARG, "unknown export selector");
   }
   if (bytes < need) return fail(c, GSR_ERR_INVALID_ARG, "destination too small");

@@ -205,10 +205,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
   return wbase + x - v;
 }
 
-// SH coefficient loads for f32 and bf16 storage.
-__device__ __forceinline__ float load_sh(const float* p, size_t i) { return __ldg(p + i); }
-__device__ __forceinline__ float load_sh(const __nv_bfloat16* p, size_t i) { return __bfloat162float(p[i]); }
-
 // Number of SMs of the current device (cached by the host and passed in).
 struct LaunchInfo {
   int num_sms;

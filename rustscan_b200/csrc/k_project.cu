@@ -2,7 +2,8 @@
 //
 // One thread per Gaussian evaluates every view of the launch: the
 // parameters are read once (the block stages its 256 x 40-byte transform
-// rows in shared memory with 128-bit loads), the thread projects the
+// rows in shared memory with 128-bit loads, and its SH rows with coalesced
+// asynchronous copies that overlap the visibility phase), the thread projects the
 // Gaussian in every view (project_forward.wgsl:19-96, project_visible.wgsl:
 // 233-310) and the block compacts the visible ones in global-id order with a
 // decoupled look-back per view, all views' look-backs at once. The tiles each visible Gaussian touches are counted
@@ -36,9 +37,44 @@ struct ProjectArgs {
   DevStatus* status;
 };
 
+// The block's SH rows live in shared memory as FP32 with an odd row stride,
+// so that the 32 threads of a warp reading coefficient j of their own rows
+// hit 32 different banks.
+template <int DEG> struct ShRows {
+  static constexpr int kN = 3 * (DEG + 1) * (DEG + 1);
+  static constexpr int kStride = kN | 1;
+  static constexpr size_t kBytes = sizeof(float) * kProjThreads * kStride;
+};
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Stages the SH rows of Gaussians g0 .. g0 + rows - 1 (global element order,
+// coalesced). FP32 rows are copied asynchronously (completed by
+// sh_rows_wait); BF16 rows are widened on the way.
+template <int DEG>
+__device__ __forceinline__ void sh_rows_issue(const float* sh, uint32_t g0, uint32_t rows, float* s_sh) {
+  using L = ShRows<DEG>;
+  const float* src = sh + (size_t)g0 * L::kN;
+  for (uint32_t e = threadIdx.x; e < rows * L::kN; e += kProjThreads)
+    cp_async4(s_sh + (e / L::kN) * L::kStride + (e % L::kN), src + e);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int DEG>
+__device__ __forceinline__ void sh_rows_issue(const __nv_bfloat16* sh, uint32_t g0, uint32_t rows, float* s_sh) {
+  using L = ShRows<DEG>;
+  const __nv_bfloat16* src = sh + (size_t)g0 * L::kN;
+  for (uint32_t e = threadIdx.x; e < rows * L::kN; e += kProjThreads)
+    s_sh[(e / L::kN) * L::kStride + (e % L::kN)] = __bfloat162float(src[e]);
+}
+__device__ __forceinline__ void sh_rows_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <class SHT, int DEG>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
   constexpr int kWarps = kProjThreads / 32;
+  extern __shared__ float s_sh[];  // [kProjThreads][ShRows<DEG>::kStride]
   __shared__ float4 s_tr4[kProjThreads * 10 / 4];
   __shared__ uint32_t s_mask[kMaxViews][kWarps];  // visibility ballots per view and warp
   __shared__ uint32_t s_wpre[kMaxViews][kWarps];  // exclusive prefix over the warps
@@ -53,9 +89,11 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
   const bool valid = g < n;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   float* s_tr = reinterpret_cast<float*>(s_tr4);
+  const uint32_t rows = g0 < n ? min(n - g0, (uint32_t)kProjThreads) : 0u;
+  // The SH rows are needed only in phase 2; their copy overlaps phase 1.
+  sh_rows_issue<DEG>(reinterpret_cast<const SHT*>(a.sp.sh), g0, rows, s_sh);
   // Stage this block's transform rows: 256 * 10 floats, 16-byte aligned.
   {
-    const uint32_t rows = min(n - g0, (uint32_t)kProjThreads);
     const float* src = a.sp.transforms + (size_t)g0 * 10;
     if (rows == kProjThreads) {
       const float4* src4 = reinterpret_cast<const float4*>(src);
@@ -101,11 +139,11 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
     s_excl[v] = excl;
     if (part == a.parts - 1) a.b.vcount[v * 4 + 0] = excl + tot;
   }
+  sh_rows_wait();
   __syncthreads();
   // Phase 2: the visible Gaussians' records at their compact indices (the
   // projection is recomputed: the same expression on the same inputs).
-  const SHT* sh = reinterpret_cast<const SHT*>(a.sp.sh);
-  constexpr int K = (DEG + 1) * (DEG + 1);
+  const float* shg = s_sh + threadIdx.x * ShRows<DEG>::kStride;
   for (uint32_t v = 0; v < nv; ++v) {
     const uint32_t m = s_mask[v][warp];
     const bool vis = (m >> lane) & 1u;
@@ -116,8 +154,7 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
       const Cam<float> cam = cam_from_desc<float>(vd);
       const Projected<float> p =
           project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
-      const SHT* shg = sh + (size_t)g * K * 3;
-      auto coeff = [&](int k, int ch) { return load_sh(shg, k * 3 + ch); };
+      auto coeff = [&](int k, int ch) { return shg[k * 3 + ch]; };
       const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, mean), coeff);
       float4* r = slice(a.b.rec, a.b.Vcap * 3, v) + (size_t)c * 3;
       r[0] = make_float4(p.mean2d.x, p.mean2d.y, p.conic.x, p.conic.y);
@@ -131,14 +168,23 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
   epoch_end(a.ctl, epoch);
 }
 
+template <class SHT, int DEG>
+cudaError_t launch_deg(dim3 grid, cudaStream_t st, const ProjectArgs& a) {
+  const size_t bytes = ShRows<DEG>::kBytes;
+  cudaError_t e = cudaFuncSetAttribute(project_kernel<SHT, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  project_kernel<SHT, DEG><<<grid, kProjThreads, bytes, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <class SHT>
-void dispatch(int degree, dim3 grid, cudaStream_t st, const ProjectArgs& a) {
+cudaError_t dispatch(int degree, dim3 grid, cudaStream_t st, const ProjectArgs& a) {
   switch (degree) {
-    case 0: project_kernel<SHT, 0><<<grid, kProjThreads, 0, st>>>(a); break;
-    case 1: project_kernel<SHT, 1><<<grid, kProjThreads, 0, st>>>(a); break;
-    case 2: project_kernel<SHT, 2><<<grid, kProjThreads, 0, st>>>(a); break;
-    case 3: project_kernel<SHT, 3><<<grid, kProjThreads, 0, st>>>(a); break;
-    default: project_kernel<SHT, 4><<<grid, kProjThreads, 0, st>>>(a); break;
+    case 0: return launch_deg<SHT, 0>(grid, st, a);
+    case 1: return launch_deg<SHT, 1>(grid, st, a);
+    case 2: return launch_deg<SHT, 2>(grid, st, a);
+    case 3: return launch_deg<SHT, 3>(grid, st, a);
+    default: return launch_deg<SHT, 4>(grid, st, a);
   }
 }
 
@@ -166,11 +212,7 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
   a.status = s.status;
   if ((uint64_t)a.parts * vs.n_views > s.lb_states_words) return cudaErrorInvalidValue;
   dim3 grid(a.parts);
-  if (sp.sh_bf16)
-    dispatch<__nv_bfloat16>(sp.degree, grid, st, a);
-  else
-    dispatch<float>(sp.degree, grid, st, a);
-  return cudaGetLastError();
+  return sp.sh_bf16 ? dispatch<__nv_bfloat16>(sp.degree, grid, st, a) : dispatch<float>(sp.degree, grid, st, a);
 }
 
 }  // namespace gsr

@@ -38,6 +38,7 @@ namespace {
 // backward amortises its per-Gaussian warp reduction over twice the pixels
 // with 4 where the tile is tall enough for an 8 x 16 warp block (16x16).
 constexpr int kFwdPPL = 2;
+static_assert(4 * kFwdPPL == 8, "forward warp blocks, and so the exported hit bits, are 8x8 pixels");
 constexpr int kBwdPPL16 = 4;
 
 struct RasterArgs {
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
       uint32_t bits = 0;
 #pragma unroll
       for (int w = 0; w < NW; ++w) bits |= (uint32_t)s_hit[w][j] << w;
-      hitw[b0 + j] = (uint8_t)bits;
+      hitw[b0 + j] = (uint8_t)bits;  // bit w: the 8x8 block of warp w
       if (bits) vis[s_cidx[j]] = 1;
     }
     if (__syncthreads_and(all_done)) break;

@@ -25,6 +25,7 @@ def run_gpu_forward(ctx, splats, cams):
             last=ctx.export(v, "last").reshape(H, W),
             ncontrib=ctx.export(v, "ncontrib").reshape(H, W),
             nvisit=ctx.export(v, "nvisit").reshape(H, W),
+            hit_blocks=ctx.export(v, "hit_blocks"),
             image=imgs[v].cpu().numpy(),
             visible=vis[v].cpu().numpy(),
         )
@@ -52,6 +53,21 @@ def assert_forward_parity(g, o, img_atol=1e-5):
     np.testing.assert_array_equal(g["last"], o.last)
     np.testing.assert_array_equal(g["nvisit"], o.nvisit)
     np.testing.assert_array_equal(g["visible"], o.visible)
+    if "hit_blocks" in g:
+        # Per-entry 8x8 blocks that took the Gaussian, defined up to each
+        # tile's largest last-contributor index.
+        H, W = o.last.shape
+        tw, th = o.tile
+        tiles_x = (W + tw - 1) // tw
+        ys, xs = np.mgrid[0:H, 0:W]
+        tile_of_pix = (ys // th) * tiles_x + (xs // tw)
+        tile_max = np.zeros(o.tiles_x * o.tiles_y, np.int64)
+        np.maximum.at(tile_max, tile_of_pix.reshape(-1), o.last.reshape(-1).astype(np.int64))
+        defined = np.arange(I) < tile_max[o.isect_tile]
+        ref = o.hit_blocks()
+        assert ref.max(initial=0) < 256
+        np.testing.assert_array_equal(g["hit_blocks"][defined], ref[defined].astype(np.uint8))
+        assert not ref[~defined].any()
     np.testing.assert_allclose(g["tfinal"], o.tfinal, rtol=0, atol=img_atol)
     np.testing.assert_allclose(g["image"], o.image, rtol=0, atol=img_atol)
 
