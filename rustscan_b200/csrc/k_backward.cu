@@ -102,8 +102,60 @@ constexpr int kGT = 128;
 template <int K> struct GatherSmem {
   static constexpr int kSh = 3 * K + 1;  // odd stride: conflict-free rows
   static constexpr int kTr = 11;
-  static constexpr size_t kBytes = sizeof(float) * (kGT * kSh + kGT * kTr);
+  static constexpr size_t kPairOff = sizeof(float) * (kGT * kSh + kGT * kTr);  // a multiple of 16
+  static constexpr size_t kBytes = kPairOff + sizeof(float4) * 2 * 6 * kGT;   // + two stages of pair records
 };
+
+__device__ __forceinline__ void cp_async16(float4* dst, const float4* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Starts the copy of this thread's six pair records of view v (compact index
+// c, none if c < 0) into its slots of stage `stage`; one commit group per
+// view whether or not it copies anything.
+__device__ __forceinline__ void pair_issue(const FwdBufs& b, uint32_t v, int32_t c, float4* s_pair, int stage,
+                                           uint32_t r) {
+  if (c >= 0) {
+    const float4* P = slice(b.pair, b.Vcap * 6, v) + c;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) cp_async16(s_pair + (stage * 6 + q) * kGT + r, P + q * b.Vcap);
+  }
+  cp_async_commit();
+}
+
+// Copies rows x NSH SH values (global element order, coalesced) into
+// shared-memory rows of stride STR as FP32. All of a thread's loads are in
+// flight at once: asynchronous copies for FP32, a batch of register loads
+// for BF16.
+template <int NSH, int STR>
+__device__ __forceinline__ void stage_sh_rows(const float* src, uint32_t rows, float* s_row) {
+  for (uint32_t e = threadIdx.x; e < rows * NSH; e += kGT) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(s_row + (e / NSH) * STR + (e % NSH));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + e) : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+template <int NSH, int STR>
+__device__ __forceinline__ void stage_sh_rows(const __nv_bfloat16* src, uint32_t rows, float* s_row) {
+  constexpr int kB = 8;
+  const uint32_t total = rows * NSH;
+  for (uint32_t e0 = threadIdx.x; e0 < total; e0 += kB * kGT) {
+    float x[kB];
+#pragma unroll
+    for (int i = 0; i < kB; ++i) {
+      const uint32_t e = e0 + i * kGT;
+      x[i] = e < total ? __bfloat162float(src[e]) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kB; ++i) {
+      const uint32_t e = e0 + i * kGT;
+      if (e < total) s_row[(e / NSH) * STR + (e % NSH)] = x[i];
+    }
+  }
+}
 
 template <class SHT, int DEG>
 __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArgs a) {
@@ -113,6 +165,8 @@ __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArg
   extern __shared__ float smem[];
   float* s_row = smem;                 // [kGT][kSh]: SH values, then SH gradients
   float* s_tg = smem + kGT * L::kSh;   // [kGT][kTr]: transform + opacity gradients
+  // [2][6][kGT]: each thread's pair records of the current and the next view
+  float4* s_pair = reinterpret_cast<float4*>(reinterpret_cast<char*>(smem) + L::kPairOff);
   const uint32_t n = a.sp.n;
   const uint32_t nv = a.vs.n_views;
   const float sc = a.grad_scale;
@@ -124,10 +178,7 @@ __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArg
     const uint32_t g = g0 + r;
     const bool own = r < rows;
     __syncthreads();
-    if (dir_term) {
-      const SHT* src = sh + (size_t)g0 * NSH;
-      for (uint32_t e = r; e < rows * NSH; e += kGT) s_row[(e / NSH) * L::kSh + (e % NSH)] = to_f(src[e]);
-    }
+    if (dir_term) stage_sh_rows<NSH, L::kSh>(sh + (size_t)g0 * NSH, rows, s_row);
     __syncthreads();
     V3<float> mean{0.f, 0.f, 0.f};
     if (own && dir_term) {
@@ -147,16 +198,25 @@ __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArg
 #pragma unroll
       for (int k = 0; k < 9; ++k) ac[k] = a.acc[k * (size_t)n + g];
     }
-    int32_t c_next = (own && nv > 0) ? a.b.c_of_gid[g] : -1;
+    // The pair records of view v + 1 are in flight while view v is summed
+    // (each thread copies and reads only its own slots).
+    int32_t c_cur = (own && nv > 0) ? a.b.c_of_gid[g] : -1;
+    if (nv > 0) pair_issue(a.b, 0, c_cur, s_pair, 0, r);
+    int32_t c_nxt = (own && nv > 1) ? slice(a.b.c_of_gid, a.b.Ncap, 1)[g] : -1;
     for (uint32_t v = 0; v < nv; ++v) {
-      const int32_t c = c_next;
-      if (v + 1 < nv) c_next = own ? slice(a.b.c_of_gid, a.b.Ncap, v + 1)[g] : -1;
+      const int32_t c = c_cur;
+      if (v + 1 < nv)
+        pair_issue(a.b, v + 1, c_nxt, s_pair, (v + 1) & 1, r);
+      else
+        cp_async_commit();
+      c_cur = c_nxt;
+      c_nxt = (own && v + 2 < nv) ? slice(a.b.c_of_gid, a.b.Ncap, v + 2)[g] : -1;
+      cp_async_wait1();  // view v's records have landed
       float st[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       float g2d = 0.f, gcol = 0.f, visf = 0.f;
       if (c >= 0) {
-        const float4* P = slice(a.b.pair, a.b.Vcap * 6, v) + c;
-        const size_t cap = a.b.Vcap;
-        const float4 q0 = P[0], q1 = P[cap], q2 = P[2 * cap], q3 = P[3 * cap], q4 = P[4 * cap], q5 = P[5 * cap];
+        const float4* P = s_pair + (v & 1) * 6 * kGT + r;
+        const float4 q0 = P[0], q1 = P[kGT], q2 = P[2 * kGT], q3 = P[3 * kGT], q4 = P[4 * kGT], q5 = P[5 * kGT];
         V3<float> vm{q0.x, q0.y, q0.z};
         const V3<float> dir{q3.x, q3.y, q3.z};
         if (dir_term) {
@@ -186,11 +246,11 @@ __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArg
           sg[k * 3 + 0] += s0;
           sg[k * 3 + 1] += s1;
           sg[k * 3 + 2] += s2;
-          csum += (fabsf(s0) + fabsf(s1) + fabsf(s2)) / 3.0f;
+          csum += fabsf(s0) + fabsf(s1) + fabsf(s2);
         }
         // Densification quantities of this view (engine/trainer.rs:660-727).
         g2d = (fabsf(vm.x) + fabsf(vm.y) + fabsf(vm.z)) / 3.0f;
-        gcol = csum / (float)K;
+        gcol = csum * (1.0f / (float)(3 * K));  // mean over coefficients of the channel mean
         // project_backwards.wgsl:192-205, 274-277.
         st[0] = q5.x;
         st[1] = q5.y;
