@@ -295,6 +295,11 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   // per tile: the tile ranges and the tile sort's digit histograms follow
   // from those counts (no histogram pass, no ranges pass).
   const bool tile_counts = vs.max_tiles <= kHistMaxTiles;
+  // With tile counts from emission and no deterministic bookkeeping, an
+  // intersection whose tile id and compact index fit in 32 bits together is
+  // one packed key (tile id high, index low), sorted alone.
+  const int tbits = bits_for(vs.max_tiles), ibits = bits_for(sp->n);
+  b.pack_bits = (tile_counts && !c->cfg.deterministic && tbits + ibits <= 32) ? (uint32_t)ibits : 0u;
   if (tile_counts) {
     GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, st));
     GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, st));
@@ -302,9 +307,12 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
     GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));
   }
   prof_mark(c, kStTileSort, st);
-  GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, b.isect_val_raw, b.isect_key, b.isect_val, b.key_tmp, b.val_tmp,
-                               b.Icap, n_views, b.vcount + 1, 4, 0, b.Icap, bits_for(vs.max_tiles), c->s, st,
-                               tile_counts));
+  if (b.pack_bits)
+    GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, nullptr, b.isect_key, nullptr, b.key_tmp, nullptr, b.Icap, n_views,
+                                 b.vcount + 1, 4, 0, b.Icap, tbits, c->s, st, true, b.pack_bits));
+  else
+    GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, b.isect_val_raw, b.isect_key, b.isect_val, b.key_tmp, b.val_tmp,
+                                 b.Icap, n_views, b.vcount + 1, 4, 0, b.Icap, tbits, c->s, st, tile_counts));
   if (c->cfg.deterministic) GSR_CUDA(c, launch_remap(vs, b, c->s, st));
   prof_mark(c, kStRanges, st);
   if (!tile_counts) GSR_CUDA(c, launch_ranges(vs, b, c->s, st));
@@ -510,8 +518,19 @@ gsr_status gsr_export(gsr_ctx* c, uint32_t view, int32_t what, void* dst, uint64
     }
     case 1: src = slice(b.gid_of_c, b.Vcap, view); need = 4 * V; break;
     case 2: src = slice(b.perm, b.Vcap, view); need = 4 * V; break;
-    case 3: src = slice(b.isect_key, b.Icap, view); need = 4 * I; break;
-    case 4: src = slice(b.isect_val, b.Icap, view); need = 4 * I; break;
+    case 3:
+    case 4:
+      if (b.pack_bits) {
+        // Packed keys: unpacked into the (idle) sort double buffers first.
+        uint32_t* tiles = slice(b.key_tmp, std::max(b.Vcap, b.Icap), view);
+        uint32_t* idx = slice(b.val_tmp, std::max(b.Vcap, b.Icap), view);
+        GSR_CUDA(c, launch_unpack_isects(b, view, (uint32_t)I, tiles, idx, st));
+        src = what == 3 ? tiles : idx;
+      } else {
+        src = what == 3 ? slice(b.isect_key, b.Icap, view) : slice(b.isect_val, b.Icap, view);
+      }
+      need = 4 * I;
+      break;
     case 5: src = slice(b.ranges, 2 * b.Tcap, view); need = 8 * T; break;
     case 6: src = slice(b.tfinal, b.Pcap, view); need = 4 * P; break;
     case 7: src = slice(b.last, b.Pcap, view); need = 4 * P; break;

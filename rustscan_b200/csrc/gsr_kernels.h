@@ -23,8 +23,8 @@ struct FwdBufs {
   uint32_t* count;         // [V] tile count of c
   uint32_t* offset;        // [V] first intersection of rank r
   int32_t* c_of_gid;       // [N] compact index of a global id, -1 if culled
-  uint32_t* isect_key;     // [I] tile id, sorted
-  uint32_t* isect_val;     // [I] compact index, sorted
+  uint32_t* isect_key;     // [I] tile id, sorted (packed: tile id << pack_bits | compact index)
+  uint32_t* isect_val;     // [I] compact index, sorted (unused when packed)
   uint32_t* isect_key_raw; // [I] emission order
   uint32_t* isect_val_raw;
   uint32_t* ranges;        // [2T]
@@ -41,7 +41,16 @@ struct FwdBufs {
   uint32_t* inv_perm;      // [I] emission index -> sorted position (deterministic mode)
   uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
   uint64_t Vcap, Ncap, Icap, Tcap, Pcap;
+  uint32_t pack_bits;      // > 0: intersections are packed keys (see isect_key), else (tile, index) pairs
 };
+
+// The compact index of intersection s (packed keys or pairs).
+__device__ __forceinline__ const uint32_t* isect_index_src(const FwdBufs& b, uint32_t v) {
+  return b.pack_bits ? b.isect_key + (size_t)b.Icap * v : b.isect_val + (size_t)b.Icap * v;
+}
+__device__ __forceinline__ uint32_t isect_index_mask(const FwdBufs& b) {
+  return b.pack_bits ? (1u << b.pack_bits) - 1u : 0xffffffffu;
+}
 
 struct ViewSet {
   const ViewDesc* views;  // device
@@ -82,13 +91,15 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
 
 // Stable LSD radix sort of (key, value) pairs in `segments` segments of
 // seg_stride elements; segment i holds counts[i * count_stride] elements
-// (or n_host when counts is null). vals_in == nullptr means values 0..n-1.
-// The result lands in keys_out/vals_out; tmp buffers are clobbered.
+// (or n_host when counts is null). vals_in == nullptr means values 0..n-1;
+// vals_out == nullptr sorts the keys alone. The digits are `bits` bits
+// from bit shift0 up. The result lands in keys_out/vals_out; tmp buffers
+// are clobbered.
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
                              uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
                              uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st,
-                             bool hist_ready = false);
+                             bool hist_ready = false, uint32_t shift0 = 0);
 
 // Bounded-wait self-test: a look-back whose predecessor never publishes
 // (look-back states 0 and 1 are overwritten); gives up after max_polls.
@@ -117,6 +128,10 @@ cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int det
 constexpr uint32_t kHistMaxTiles = 8192;
 cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
 cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+// Packed mode only: intersections [0, n) of a view as separate tile ids and
+// compact indices.
+cudaError_t launch_unpack_isects(const FwdBufs& b, uint32_t view, uint32_t n, uint32_t* tiles, uint32_t* vals,
+                                 cudaStream_t st);
 cudaError_t launch_remap(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_ranges(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 

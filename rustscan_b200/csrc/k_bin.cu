@@ -145,11 +145,14 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
         const uint64_t o = (uint64_t)S.off[owner] + S.run[owner] + (uint32_t)__popc(before);
         if (o < cap) {
           if (HIST) atomicAdd(&s_th[tx + ty * vd.tiles_x], 1u);
-          keys[o] = tx + ty * vd.tiles_x;
-          if (det) {
+          if (b.pack_bits) {
+            keys[o] = ((tx + ty * vd.tiles_x) << b.pack_bits) | S.cid[owner];
+          } else if (det) {
+            keys[o] = tx + ty * vd.tiles_x;
             vals[o] = (uint32_t)o;
             emit_c[o] = S.cid[owner];
           } else {
+            keys[o] = tx + ty * vd.tiles_x;
             vals[o] = S.cid[owner];
           }
         }
@@ -239,6 +242,17 @@ __global__ void __launch_bounds__(256) remap_kernel(FwdBufs b) {
     const uint32_t c = inv[e];
     inv[e] = s;
     vals[s] = c;
+  }
+}
+
+// Packed intersections of one view back to (tile id, compact index) pairs
+// (inspection exports).
+__global__ void __launch_bounds__(256) unpack_isects_kernel(const uint32_t* packed, uint32_t n, uint32_t bits,
+                                                            uint32_t* tiles, uint32_t* vals) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const uint32_t k = packed[s];
+    tiles[s] = k >> bits;
+    vals[s] = k & ((1u << bits) - 1u);
   }
 }
 
@@ -340,6 +354,14 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
 cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
   tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_isects(const FwdBufs& b, uint32_t view, uint32_t n, uint32_t* tiles, uint32_t* vals,
+                                 cudaStream_t st) {
+  if (!b.pack_bits || n == 0) return cudaSuccess;
+  const uint32_t blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+  unpack_isects_kernel<<<blocks, 256, 0, st>>>(slice(b.isect_key, b.Icap, view), n, b.pack_bits, tiles, vals);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ namespace {
 
 constexpr int LTX = 32, LTY = 32, R = 5, WIN = 11;
 constexpr int HX = LTX + 2 * R, HY = LTY + 2 * R;
+constexpr int kLT = 256;                          // threads per loss block
+constexpr int kHaloIt = (HX * HY + kLT - 1) / kLT;  // halo elements per thread
 
 struct LossArgs {
   const ViewDesc* views;
@@ -49,7 +51,7 @@ struct SsimFwdSmem {
   float red[2][8];
 };
 
-__global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
+__global__ void __launch_bounds__(kLT) ssim_fwd_kernel(LossArgs a) {
   extern __shared__ float4 smem_raw[];
   SsimFwdSmem& S = *reinterpret_cast<SsimFwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
@@ -61,16 +63,33 @@ __global__ void __launch_bounds__(256) ssim_fwd_kernel(LossArgs a) {
   const int x0 = (tile % tiles_x) * LTX, y0 = (tile / tiles_x) * LTY;
   const float* pred = a.pred + vd.pix_base * 4;
   const float* tgt = a.target + vd.pix_base * 3;
-  for (int i = threadIdx.x; i < HX * HY; i += blockDim.x) {
-    const int hy = i / HX, hx = i % HX;
-    const int gx = clampi(x0 + hx - R, 0, W - 1), gy = clampi(y0 + hy - R, 0, H - 1);
-    const size_t p = (size_t)gy * W + gx;
-    const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
-    S.p[0][hy][hx] = x;
-    S.p[1][hy][hx] = y;
-    S.p[2][hy][hx] = x * x;
-    S.p[3][hy][hx] = y * y;
-    S.p[4][hy][hx] = x * y;
+  {
+    // All of a thread's halo loads are issued before the first store.
+    float xs[kHaloIt], ys[kHaloIt];
+#pragma unroll
+    for (int it = 0; it < kHaloIt; ++it) {
+      const int i = threadIdx.x + it * kLT;
+      if (i < HX * HY) {
+        const int hy = i / HX, hx = i % HX;
+        const int gx = clampi(x0 + hx - R, 0, W - 1), gy = clampi(y0 + hy - R, 0, H - 1);
+        const size_t p = (size_t)gy * W + gx;
+        xs[it] = pred[p * 4 + ch];
+        ys[it] = tgt[p * 3 + ch];
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < kHaloIt; ++it) {
+      const int i = threadIdx.x + it * kLT;
+      if (i < HX * HY) {
+        const int hy = i / HX, hx = i % HX;
+        const float x = xs[it], y = ys[it];
+        S.p[0][hy][hx] = x;
+        S.p[1][hy][hx] = y;
+        S.p[2][hy][hx] = x * x;
+        S.p[3][hy][hx] = y * y;
+        S.p[4][hy][hx] = x * y;
+      }
+    }
   }
   __syncthreads();
   // Horizontal pass: every halo row, output columns in pairs.
@@ -184,7 +203,7 @@ struct SsimBwdSmem {
   float v[3][LTY][HX];
 };
 
-__global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
+__global__ void __launch_bounds__(kLT) ssim_bwd_kernel(LossArgs a) {
   extern __shared__ float4 smem_raw[];
   SsimBwdSmem& S = *reinterpret_cast<SsimBwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
@@ -195,13 +214,46 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
   if (tile >= tiles_x * tiles_y) return;
   const int x0 = (tile % tiles_x) * LTX, y0 = (tile / tiles_x) * LTY;
   const float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
-  for (int i = threadIdx.x; i < HX * HY; i += blockDim.x) {
-    const int hy = i / HX, hx = i % HX;
-    const int gx = x0 + hx - R, gy = y0 + hy - R;
-    const bool ok = gx >= 0 && gx < W && gy >= 0 && gy < H;
-    const size_t p = (size_t)gy * W + gx;
+  const float* pred = a.pred + vd.pix_base * 4;
+  const float* tgt = a.target + vd.pix_base * 3;
+  // The prediction and target values of this thread's output pixels (read
+  // at the end) are loaded now, with the halo of the three maps.
+  constexpr int kOutIt = LTY * (LTX / 2) / kLT;
+  float px_x[kOutIt][2], px_y[kOutIt][2];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) S.g[m][hy][hx] = ok ? maps[m * a.Pcap + p] : 0.f;
+  for (int it = 0; it < kOutIt; ++it) {
+    const int i = threadIdx.x + it * kLT;
+    const int oy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int px = x0 + ox + c, py = y0 + oy;
+      const bool ok = px < W && py < H;
+      const size_t p = (size_t)py * W + px;
+      px_x[it][c] = ok ? pred[p * 4 + ch] : 0.f;
+      px_y[it][c] = ok ? tgt[p * 3 + ch] : 0.f;
+    }
+  }
+  {
+    float gs[kHaloIt][3];
+#pragma unroll
+    for (int it = 0; it < kHaloIt; ++it) {
+      const int i = threadIdx.x + it * kLT;
+      const int hy = i / HX, hx = i % HX;
+      const int gx = x0 + hx - R, gy = y0 + hy - R;
+      const bool ok = i < HX * HY && gx >= 0 && gx < W && gy >= 0 && gy < H;
+      const size_t p = (size_t)gy * W + gx;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) gs[it][m] = ok ? maps[m * a.Pcap + p] : 0.f;
+    }
+#pragma unroll
+    for (int it = 0; it < kHaloIt; ++it) {
+      const int i = threadIdx.x + it * kLT;
+      if (i < HX * HY) {
+        const int hy = i / HX, hx = i % HX;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) S.g[m][hy][hx] = gs[it][m];
+      }
+    }
   }
   __syncthreads();
   // Adjoint of the vertical pass: tile rows, all halo columns (in pairs).
@@ -225,12 +277,12 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
     for (int m = 0; m < 3; ++m) *reinterpret_cast<float2*>(&S.v[m][oy][hx]) = acc[m];
   }
   __syncthreads();
-  const float* pred = a.pred + vd.pix_base * 4;
-  const float* tgt = a.target + vd.pix_base * 3;
   float* out = a.v_pred + vd.pix_base * 4;
   const float M = 3.f * (float)W * (float)H;
   const float kl = a.l1_w / M, ks = -a.ssim_w / M;
-  for (int i = threadIdx.x; i < LTY * (LTX / 2); i += blockDim.x) {
+#pragma unroll
+  for (int it = 0; it < kOutIt; ++it) {
+    const int i = threadIdx.x + it * kLT;
     const int oy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
     const int px = x0 + ox, py = y0 + oy;
     if (px >= W || py >= H) continue;
@@ -270,7 +322,7 @@ __global__ void __launch_bounds__(256) ssim_bwd_kernel(LossArgs a) {
       if (pc >= W) continue;
       const float a0 = c ? acc[0].y : acc[0].x, a1 = c ? acc[1].y : acc[1].x, a2 = c ? acc[2].y : acc[2].x;
       const size_t p = (size_t)py * W + pc;
-      const float x = pred[p * 4 + ch], y = tgt[p * 3 + ch];
+      const float x = px_x[it][c], y = px_y[it][c];
       const float dlt = x - y;
       const float sg = dlt > 0.f ? 1.f : (dlt < 0.f ? -1.f : 0.f);
       out[p * 4 + ch] = kl * sg + ks * (a0 + 2.f * x * a1 + y * a2);
@@ -355,8 +407,8 @@ cudaError_t launch_loss(const ViewSet& vs, const ViewDesc* host_views, const flo
   // More than the 48 KB default of dynamic shared memory (set for the current device).
   cudaFuncSetAttribute(ssim_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SsimFwdSmem));
   cudaFuncSetAttribute(ssim_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SsimBwdSmem));
-  ssim_fwd_kernel<<<grid, 256, sizeof(SsimFwdSmem), st>>>(a);
-  ssim_bwd_kernel<<<grid, 256, sizeof(SsimBwdSmem), st>>>(a);
+  ssim_fwd_kernel<<<grid, kLT, sizeof(SsimFwdSmem), st>>>(a);
+  ssim_bwd_kernel<<<grid, kLT, sizeof(SsimBwdSmem), st>>>(a);
   loss_reduce_kernel<<<vs.n_views, 256, 0, st>>>(a, vs.n_views, loss);
   return cudaGetLastError();
 }

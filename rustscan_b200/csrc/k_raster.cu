@@ -184,7 +184,8 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   const float pcx = (float)px + 0.5f;
   const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
   const uint32_t s0 = ranges[2 * t], s1 = ranges[2 * t + 1];
-  const uint32_t* vals = slice(a.b.isect_val, a.b.Icap, v);
+  const uint32_t* vals = isect_index_src(a.b, v);
+  const uint32_t vmask = isect_index_mask(a.b);
   const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
   uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
   uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     const uint32_t nb = min((uint32_t)BATCH, s1 - b0);
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < nb; j += NT) {
-      const uint32_t c = vals[b0 + j];
+      const uint32_t c = vals[b0 + j] & vmask;
       float4 A, B, Cc;
       s_mask[j] = (uint8_t)stage_one<TW, PPL, NW, true>(rec, c, tx0, ty0, A, B, Cc);
       s_a[j] = A;
@@ -500,7 +501,8 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   const float pcx = (float)px + 0.5f;
   const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
   const uint32_t s0 = ranges[2 * t];
-  const uint32_t* vals = slice(a.b.isect_val, a.b.Icap, v);
+  const uint32_t* vals = isect_index_src(a.b, v);
+  const uint32_t vmask = isect_index_mask(a.b);
   const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
   const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
   float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
@@ -529,7 +531,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
       const uint32_t hm = hit_bits_for<TW, TH, PPL>(hitw[bs + j]);
       s_mask[j] = (uint8_t)hm;
       if (hm) {
-        const uint32_t c = vals[bs + j];
+        const uint32_t c = vals[bs + j] & vmask;
         float4 A, B, Cc;
         (void)stage_one<TW, PPL, NW, false>(rec, c, tx0, ty0, A, B, Cc);
         s_a[j] = A;

@@ -12,9 +12,11 @@
 //    back across partitions for their global offsets, then scatter through
 //    shared memory so that every digit's run is written contiguously;
 //  - scans are single-pass with the same look-back.
-// Keys are u32; `bits` limits the passes (8 bits each). Stability (ties in
-// input order) is what the reference's index tie-break provides
-// (radix_sort.wgsl:21-26).
+// Keys are u32; `bits` limits the passes (8 bits each, starting at bit
+// shift0). Stability (ties in input order) is what the reference's index
+// tie-break provides (radix_sort.wgsl:21-26). Without values, the keys are
+// sorted alone (the binning packs tile id and compact index into one key
+// when both fit in 32 bits).
 #include "gsr_kernels.h"
 
 namespace gsr {
@@ -36,7 +38,8 @@ __device__ __forceinline__ uint32_t seg_count(const uint32_t* counts, uint32_t s
 
 __global__ void __launch_bounds__(256) sort_hist_kernel(const uint32_t* keys, uint64_t seg_stride,
                                                         const uint32_t* counts, uint32_t count_stride,
-                                                        uint32_t n_host, uint64_t cap, int passes, uint32_t* hist) {
+                                                        uint32_t n_host, uint64_t cap, int passes, uint32_t shift0,
+                                                        uint32_t* hist) {
   __shared__ uint32_t h[4][256];
   for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -45,7 +48,7 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(const uint32_t* keys, ui
   const uint32_t* k = keys + (size_t)seg * seg_stride;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t key = k[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(key >> (8 * p)) & 255u], 1u);
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(key >> (shift0 + 8 * p)) & 255u], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
@@ -81,9 +84,11 @@ struct SortPassArgs {
   DevStatus* status;
 };
 
+// KV: values travel with the keys; otherwise the keys are sorted alone.
+template <bool KV>
 __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a) {
   __shared__ uint32_t s_keys[kSortTile];
-  __shared__ uint32_t s_vals[kSortTile];
+  __shared__ uint32_t s_vals[KV ? kSortTile : 1];
   __shared__ uint32_t s_whist[kSortWarps][256];
   __shared__ uint32_t s_dstart[256];
   __shared__ uint32_t s_gbase[256];
@@ -110,7 +115,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       const bool ok = idx < n;
       key[i] = ok ? kin[idx] : 0xffffffffu;
-      val[i] = ok ? (vin ? vin[idx] : idx) : 0u;
+      val[i] = (KV && ok) ? (vin ? vin[idx] : idx) : 0u;
     }
     for (int j = lane; j < 256; j += 32) s_whist[warp][j] = 0;
     __syncwarp();
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
         const uint32_t dd = (key[i] >> a.shift) & 255u;
         const uint32_t pos = s_dstart[dd] + s_whist[warp][dd] + lrank[i];
         s_keys[pos] = key[i];
-        s_vals[pos] = val[i];
+        if (KV) s_vals[pos] = val[i];
       }
     }
     __syncthreads();
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
       const uint32_t k = s_keys[j];
       const uint32_t dst = s_gbase[(k >> a.shift) & 255u] + j;
       kout[dst] = k;
-      vout[dst] = s_vals[j];
+      if (KV) vout[dst] = s_vals[j];
     }
   }
   epoch_end(a.ctl, epoch);
@@ -266,8 +271,10 @@ int persistent_blocks(int num_sms, uint32_t segments, int per_sm) {
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride, uint32_t segments,
                              const uint32_t* counts, uint32_t count_stride, uint32_t n_host, uint64_t cap_per_segment,
-                             int bits, const Scratch& s, cudaStream_t st, bool hist_ready) {
+                             int bits, const Scratch& s, cudaStream_t st, bool hist_ready, uint32_t shift0) {
   if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
+  if (shift0 >= 32 || (keys_in == nullptr)) return cudaErrorInvalidValue;
+  const bool kv = vals_out != nullptr;
   int passes = (bits + 7) / 8;
   if (passes < 1) passes = 1;
   if (passes > 4) passes = 4;
@@ -278,7 +285,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     if (e != cudaSuccess) return e;
     dim3 grid(persistent_blocks(s.num_sms, segments, 4), segments);
     sort_hist_kernel<<<grid, 256, 0, st>>>(keys_in, seg_stride, counts, count_stride, n_host, cap_per_segment, passes,
-                                           s.hist);
+                                           shift0, s.hist);
   }
   sort_hist_scan_kernel<<<dim3(passes, segments), 256, 0, st>>>(s.hist, s.hist_base);
   // Ping-pong so that the last pass writes keys_out/vals_out.
@@ -298,7 +305,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.count_stride = count_stride;
     a.n_host = n_host;
     a.cap = cap_per_segment;
-    a.shift = 8 * p;
+    a.shift = shift0 + 8 * p;
     a.pass = p;
     a.base = s.hist_base;
     a.states = s.lb_states;
@@ -306,7 +313,10 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.ctl = s.ctl;
     a.status = s.status;
     dim3 grid(persistent_blocks(s.num_sms, segments, 3), segments);
-    sort_pass_kernel<<<grid, kSortThreads, 0, st>>>(a);
+    if (kv)
+      sort_pass_kernel<true><<<grid, kSortThreads, 0, st>>>(a);
+    else
+      sort_pass_kernel<false><<<grid, kSortThreads, 0, st>>>(a);
     ki = ko;
     vi = vo;
   }
