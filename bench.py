@@ -281,7 +281,8 @@ def profile_step(args):
     sc = S.config3(n=args.n, views=args.views)
     cams = sc.cameras
     H, W = cams[0].height, cams[0].width
-    ctx = make_context(args.n, len(cams))
+    # The tile shape and raster batch the autotuner picks on this workload.
+    ctx = make_context(args.n, len(cams), tile=(16, 16), batch=128)
     splats = host_splats_to_device(sc)
     fit_capacity(ctx, splats, cams)
     rng = np.random.default_rng(0)

@@ -348,8 +348,7 @@ struct BwdPair {
   uint32_t last0, last1;
   float2 T, K;          // transmittance, background term
   float2 S0, S1, S2;    // colour accumulated behind the current Gaussian
-  float2 vr, vg, vb;
-  float2 npcy;
+  float2 vr, vg, vb;    // upstream colour gradient
 };
 
 __device__ __forceinline__ void load_bwd_pair(const RasterArgs& a, const ViewDesc& vd, uint32_t v, uint32_t px,
@@ -377,7 +376,6 @@ __device__ __forceinline__ void load_bwd_pair(const RasterArgs& a, const ViewDes
   p.vr = make_float2(g[0][0], g[1][0]);
   p.vg = make_float2(g[0][1], g[1][1]);
   p.vb = make_float2(g[0][2], g[1][2]);
-  p.npcy = make_float2(-((float)py0 + 0.5f), -((float)(py0 + 4) + 0.5f));
 }
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -386,28 +384,45 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+// A lane's sums over its pixels for the current Gaussian. With dx shared
+// by the lane's column and vs the gradient with respect to sigma at each
+// pixel, the mean and conic gradient sums factor through three moments:
+//   sum vs (a dx + b dy) = a dx M0 + b M1,   sum vs dx^2 / 2 = dx^2 / 2 M0,
+//   sum vs dx dy = dx M1,                    sum vs dy^2 / 2 = M2 / 2,
+// with M0 = sum vs, M1 = sum vs dy, M2 = sum vs dy^2. The absolute
+// mean-gradient sums (densification statistics) stay per pixel.
+struct BwdAcc {
+  float2 m0, m1, m2;
+  float2 cr, cg, cb;  // colour gradients
+  float2 op;          // opacity-path gradient
+  float ax, ay;       // sums of |d/dx| and |d/dy| of the per-pixel mean gradients
+  uint32_t n;         // contributing pixels
+};
+
 // One step of the reverse walk for both pixels of a pair: the contribution
 // decisions repeat the forward's bit for bit; the gradient follows
 // blend_step_grad (rasterize_backwards, exact adjoint), with the
-// transmittance recovered with a Newton-refined hardware reciprocal. Adds the pair's gradient into x[0..11) and returns, per
-// pixel, whether it counts as a contributor (in the reference semantics a
-// pixel whose transmittance fell to 1e-4 no longer does).
-__device__ __forceinline__ uint32_t bwd_pair_step(BwdPair& p, uint32_t s, float dx, float t1, float t2, float hdx2,
-                                                  const float4& A, const float4& B, const float4& Cc, int ref_mode,
-                                                  float (&x)[16]) {
+// transmittance recovered with a Newton-refined hardware reciprocal. Adds
+// the pair's terms into acc. With REF (the reference semantics) a pixel
+// whose transmittance fell to 1e-4 no longer counts as a contributor and
+// gets no gradient.
+template <bool REF>
+__device__ __forceinline__ void bwd_pair_step(BwdPair& p, float2 npcy, uint32_t s, float t1, float t2, float adx,
+                                              float bdx, float cb, const float4& A, const float4& B,
+                                              const float4& Cc, BwdAcc& acc) {
   const bool in0 = s < p.last0, in1 = s < p.last1;
-  if (!(in0 || in1)) return 0u;
-  const float2 dy = make_float2(eadd(A.y, p.npcy.x), eadd(A.y, p.npcy.y));
+  if (!(in0 || in1)) return;
+  const float2 dy = make_float2(eadd(A.y, npcy.x), eadd(A.y, npcy.y));
   const float2 sg = sigma2(t1, t2, dy, B.x);
   const bool l0 = in0 && !(sg.x > B.y), l1 = in1 && !(sg.y > B.y);
-  if (!(l0 || l1)) return 0u;
+  if (!(l0 || l1)) return;
   const float2 gs = blend_exp2(sg);
   const float2 og = mul2(f2(B.z), gs);
   const float ax = fminf(0.999f, og.x), ay = fminf(0.999f, og.y);
   const bool c0 = l0 && sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
   const bool c1 = l1 && sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
-  if (!(c0 || c1)) return 0u;
-  const bool sk0 = ref_mode && p.T.x <= 1e-4f, sk1 = ref_mode && p.T.y <= 1e-4f;
+  if (!(c0 || c1)) return;
+  const bool sk0 = REF && p.T.x <= 1e-4f, sk1 = REF && p.T.y <= 1e-4f;
   const float2 al = make_float2(ax, ay);
   const float2 am = make_float2(c0 ? ax : 0.f, c1 ? ay : 0.f);
   const float2 om = add2(f2(1.f), neg2(am));
@@ -437,25 +452,18 @@ __device__ __forceinline__ uint32_t bwd_pair_step(BwdPair& p, uint32_t s, float 
   const float2 vs = make_float2(gg0 ? -av.x : 0.f, gg1 ? -av.y : 0.f);
   const float2 vo = mul2(va, gs);
   const float2 vsdy = mul2(vs, dy);
-  const float ca = A.z, cb = 0.5f * A.w, cc = B.x;
-  const float2 vxy0 = mul2(vs, fma2(f2(cb), dy, f2(ca * dx)));
-  const float2 vxy1 = mul2(vs, fma2(f2(cc), dy, f2(cb * dx)));
-  const float2 vc0 = mul2(vs, f2(hdx2));
-  const float2 vc1 = mul2(vsdy, f2(dx));
-  const float2 vc2 = mul2(vsdy, mul2(f2(0.5f), dy));
-  const float2 vr = mul2(visg, p.vr), vg = mul2(visg, p.vg), vb = mul2(visg, p.vb);
-  x[0] += vxy0.x + vxy0.y;
-  x[1] += vxy1.x + vxy1.y;
-  x[2] += vc0.x + vc0.y;
-  x[3] += vc1.x + vc1.y;
-  x[4] += vc2.x + vc2.y;
-  x[5] += vr.x + vr.y;
-  x[6] += vg.x + vg.y;
-  x[7] += vb.x + vb.y;
-  x[8] += (gg0 ? vo.x : 0.f) + (gg1 ? vo.y : 0.f);
-  x[9] += fabsf(vxy0.x) + fabsf(vxy0.y);
-  x[10] += fabsf(vxy1.x) + fabsf(vxy1.y);
-  return (gm0 ? 1u : 0u) | (gm1 ? 2u : 0u);
+  acc.m0 = add2(acc.m0, vs);
+  acc.m1 = add2(acc.m1, vsdy);
+  acc.m2 = fma2(vsdy, dy, acc.m2);
+  const float2 vxy0 = mul2(vs, fma2(f2(cb), dy, f2(adx)));
+  const float2 vxy1 = mul2(vs, fma2(f2(B.x), dy, f2(bdx)));
+  acc.ax += fabsf(vxy0.x) + fabsf(vxy0.y);
+  acc.ay += fabsf(vxy1.x) + fabsf(vxy1.y);
+  acc.cr = fma2(visg, p.vr, acc.cr);
+  acc.cg = fma2(visg, p.vg, acc.cg);
+  acc.cb = fma2(visg, p.vb, acc.cb);
+  acc.op = add2(acc.op, make_float2(gg0 ? vo.x : 0.f, gg1 ? vo.y : 0.f));
+  acc.n += (gm0 ? 1u : 0u) + (gm1 ? 1u : 0u);
 }
 
 // Maps the forward's per-entry warp-block bits (blocks of kFwdPPL pixels
@@ -475,20 +483,31 @@ __device__ __forceinline__ uint32_t hit_bits_for(uint32_t f) {
   return m;
 }
 
-template <int TW, int TH, int PPL, int BATCH>
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// The backward walks the tile's list from its largest last-contributor
+// index down in batches. Batches are double-buffered: while batch k is
+// evaluated, the raw records of batch k + 1 are in flight (asynchronous
+// copies into the other buffer) and the list entries of batch k + 2 (hit
+// bits and compact indices) are loaded into registers.
+template <int TW, int TH, int PPL, int BATCH, bool REF>
 __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) {
   static_assert(PPL % 2 == 0, "pixels per lane come in pairs");
   static_assert(TH % (4 * PPL) == 0 && (TW * TH / PPL) % 32 == 0, "warp blocks tile the tile");
   constexpr int NT = TW * TH / PPL;
   constexpr int NW = NT / 32;
   constexpr int NP = PPL / 2;
-  __shared__ float4 s_a[BATCH];
-  __shared__ float4 s_b[BATCH];
-  __shared__ float4 s_c[BATCH];
-  __shared__ uint32_t s_cidx[BATCH];
-  __shared__ uint8_t s_mask[BATCH];
+  constexpr int kSI = (BATCH + NT - 1) / NT;  // entries a thread stages per batch
+  __shared__ float4 s_rec[2][BATCH][3];        // raw records
+  __shared__ uint32_t s_cidx[2][BATCH];
+  __shared__ uint8_t s_mask[2][BATCH];         // warp blocks that take the entry
   __shared__ uint16_t s_list[NW][BATCH];
-  __shared__ float4 s_part[NW][BATCH][3];
+  __shared__ float4 s_part[NW][BATCH][3];      // written by the warps whose bit is set
   __shared__ uint32_t s_max;
   const uint32_t item = blockIdx.x;
   const uint32_t v = find_view(a.vs, item);
@@ -507,7 +526,6 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
   float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
   float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
-  const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
   BwdPair pp[NP];
   uint32_t mylast = 0;
 #pragma unroll
@@ -521,82 +539,135 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   if (lane == 0) atomicMax(&s_max, wmax);
   __syncthreads();
   const uint32_t smax = s_max;
-  for (uint32_t be = smax; be > s0;) {
-    const uint32_t bs = (be - s0 > (uint32_t)BATCH) ? be - BATCH : s0;
-    const uint32_t nb = be - bs;
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += NT) {
-      // Only the warp blocks that took the entry in the forward can take
-      // it here; an entry no block took is not staged at all.
-      const uint32_t hm = hit_bits_for<TW, TH, PPL>(hitw[bs + j]);
-      s_mask[j] = (uint8_t)hm;
-      if (hm) {
-        const uint32_t c = vals[bs + j] & vmask;
-        float4 A, B, Cc;
-        (void)stage_one<TW, PPL, NW, false>(rec, c, tx0, ty0, A, B, Cc);
-        s_a[j] = A;
-        s_b[j] = B;
-        s_c[j] = Cc;
-        s_cidx[j] = c;
+  auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
+  // List entries [lo, hi) of a batch into registers.
+  uint32_t pc[kSI], ph[kSI];
+  auto fetch = [&](uint32_t lo, uint32_t hi) {
+#pragma unroll
+    for (int it = 0; it < kSI; ++it) {
+      const uint32_t s = lo + threadIdx.x + it * NT;
+      const bool ok = threadIdx.x + it * NT < (uint32_t)BATCH && s < hi;
+      ph[it] = ok ? hitw[s] : 0u;
+      pc[it] = ok ? (vals[s] & vmask) : 0u;
+    }
+  };
+  // Masks, indices and record copies of the fetched batch [lo, hi) into
+  // buffer `buf`; one commit group per call.
+  auto issue = [&](uint32_t lo, uint32_t hi, int buf) {
+#pragma unroll
+    for (int it = 0; it < kSI; ++it) {
+      const uint32_t j = threadIdx.x + it * NT;
+      if (j < (uint32_t)BATCH && lo + j < hi) {
+        const uint32_t hm = hit_bits_for<TW, TH, PPL>(ph[it]);
+        s_mask[buf][j] = (uint8_t)hm;
+        if (hm) {
+          s_cidx[buf][j] = pc[it];
+          const float4* r = rec + (size_t)pc[it] * 3;
+          cp_async16(&s_rec[buf][j][0], r);
+          cp_async16(&s_rec[buf][j][1], r + 1);
+          cp_async16(&s_rec[buf][j][2], r + 2);
+        }
       }
     }
-    {
-      float4* z = &s_part[0][0][0];
-      for (uint32_t q = threadIdx.x; q < (uint32_t)(NW * BATCH * 3); q += NT) z[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+    cp_async_commit();
+  };
+  uint32_t be = smax, bs = be > s0 ? batch_lo(be) : s0;
+  if (be > s0) {
+    fetch(bs, be);
+    issue(bs, be, 0);
+  }
+  uint32_t nbe = bs, nbs = nbe > s0 ? batch_lo(nbe) : s0;
+  if (nbe > s0) fetch(nbs, nbe);
+  int buf = 0;
+  while (be > s0) {
+    const uint32_t nb = be - bs;
+    if (nbe > s0)
+      issue(nbs, nbe, buf ^ 1);
+    else
+      cp_async_commit();
+    const uint32_t n2e = nbs, n2s = n2e > s0 ? batch_lo(n2e) : s0;
+    if (n2e > s0) fetch(n2s, n2e);
+    cp_async_wait1();  // this thread's copies of the current batch have landed
     __syncthreads();
     if (bs < wmax) {
-      const int cnt = build_list(s_mask, nb, warp, lane, s_list[warp]);
+      const int cnt = build_list(s_mask[buf], nb, warp, lane, s_list[warp]);
       for (int e = cnt - 1; e >= 0; --e) {
         const uint32_t j = s_list[warp][e];
         const uint32_t s = bs + j;
-        if (s >= wmax) continue;  // warp-uniform
-        const float4 A = s_a[j];
-        const float4 B = s_b[j];
-        const float4 Cc = s_c[j];
+        const float4 r0 = s_rec[buf][j][0], r1 = s_rec[buf][j][1], r2 = s_rec[buf][j][2];
+        const float4 A = make_float4(r0.x, r0.y, r0.z, 2.f * r0.w);  // 2b is exact
+        const float4 B = make_float4(r1.x, r2.y + kRejectMargin, r1.y, 0.f);
+        const float4 Cc = make_float4(r1.z, r1.w, r2.x, 0.f);
         const float dx = esub(A.x, pcx);
         const float t1 = emul(emul(A.z, dx), dx);
         const float t2 = emul(A.w, dx);
-        const float hdx2 = 0.5f * dx * dx;
-        float x[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) x[i] = 0.f;
-        uint32_t ncontrib = 0;
+        const float cb = 0.5f * A.w;
+        const float adx = A.z * dx, bdx = cb * dx;
+        BwdAcc acc;
+        acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.op = f2(0.f);
+        acc.ax = acc.ay = 0.f;
+        acc.n = 0u;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-          const uint32_t cb = bwd_pair_step(pp[k], s, dx, t1, t2, hdx2, A, B, Cc, a.ref_mode, x);
-          ncontrib += __popc(__ballot_sync(0xffffffffu, cb & 1u)) + __popc(__ballot_sync(0xffffffffu, cb & 2u));
+          const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
+          bwd_pair_step<REF>(pp[k], npcy, s, t1, t2, adx, bdx, cb, A, B, Cc, acc);
         }
-        if (ncontrib) {
-          float r = warp_reduce_scatter16(x, lane);
-          const int slot = lane >> 1;
-          // v_rgb is zero for a channel whose raw colour is negative.
-          if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
-          float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
-          if ((lane & 1) == 0 && slot < 11) sp[slot] = r;
-          if (lane == 0) sp[11] = (float)ncontrib;
-        }
+        const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
+        float x[16];
+        x[0] = adx * M0 + cb * M1;
+        x[1] = bdx * M0 + B.x * M1;
+        x[2] = (0.5f * dx * dx) * M0;
+        x[3] = dx * M1;
+        x[4] = 0.5f * M2;
+        x[5] = acc.cr.x + acc.cr.y;
+        x[6] = acc.cg.x + acc.cg.y;
+        x[7] = acc.cb.x + acc.cb.y;
+        x[8] = acc.op.x + acc.op.y;
+        x[9] = acc.ax;
+        x[10] = acc.ay;
+        x[11] = (float)acc.n;
+#pragma unroll
+        for (int i = 12; i < 16; ++i) x[i] = 0.f;
+        float r = warp_reduce_scatter16(x, lane);
+        const int slot = lane >> 1;
+        // v_rgb is zero for a channel whose raw colour is negative.
+        if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
+        float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
+        if ((lane & 1) == 0 && slot < 12) sp[slot] = r;
       }
     }
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < nb * 3; q += NT) {
       const uint32_t j = q / 3, k = q % 3;
-      float4 f = s_part[0][j][k];
+      const uint32_t m = s_mask[buf][j];
+      float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+      bool any = false;
 #pragma unroll
-      for (int w = 1; w < NW; ++w) {
+      for (int w = 0; w < NW; ++w) {
+        if (!((m >> w) & 1u)) continue;
         const float4 g = s_part[w][j][k];
-        f.x = f.x + g.x;
-        f.y = f.y + g.y;
-        f.z = f.z + g.z;
-        f.w = f.w + g.w;
+        if (!any) {
+          f = g;
+          any = true;
+        } else {
+          f.x = f.x + g.x;
+          f.y = f.y + g.y;
+          f.z = f.z + g.z;
+          f.w = f.w + g.w;
+        }
       }
       if (a.det) {
         reinterpret_cast<float4*>(part + (size_t)(bs + j) * 12)[k] = f;
       } else if (f.x != 0.f || f.y != 0.f || f.z != 0.f || f.w != 0.f) {
-        atomicAdd(sgrad + (size_t)s_cidx[j] * 3 + k, f);
+        atomicAdd(sgrad + (size_t)s_cidx[buf][j] * 3 + k, f);
       }
     }
+    __syncthreads();  // the next batch's copies reuse this buffer
     be = bs;
+    bs = nbs;
+    nbe = n2e;
+    nbs = n2s;
+    buf ^= 1;
   }
   // Deterministic mode: list entries of this tile that no pixel reached keep
   // zero partial records.
@@ -611,8 +682,9 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
 
 // Gaussians per shared-memory batch: 0 selects the tuned defaults (128 in
 // the forward, 64 in the backward); other values round up to 64, 128 or 256.
-// The backward of shapes with four warps per tile caps at 128 (its per-warp
-// partial sums would not fit the 48 KB of static shared memory).
+// The backward of shapes with two or more warps per tile caps at 128 (its
+// double-buffered records and per-warp partial sums would not fit the 48 KB
+// of static shared memory).
 inline int pick_batch(uint32_t want, int dflt) {
   if (want == 0) return dflt;
   return want <= 64 ? 64 : (want <= 128 ? 128 : 256);
@@ -628,18 +700,23 @@ cudaError_t launch_fwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch
   }
   return cudaGetLastError();
 }
-template <int TW, int TH, int PPL>
-cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
+template <int TW, int TH, int PPL, bool REF>
+cudaError_t launch_bwd_mode(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
   constexpr int NT = TW * TH / PPL;
-  constexpr int kMaxBatch = NT / 32 >= 4 ? 128 : 256;
+  constexpr int kMaxBatch = NT / 32 >= 2 ? 128 : 256;
   int b = pick_batch(batch, 64);
   if (b > kMaxBatch) b = kMaxBatch;
   switch (b) {
-    case 64: raster_bwd_kernel<TW, TH, PPL, 64><<<items, NT, 0, st>>>(a); break;
-    case 128: raster_bwd_kernel<TW, TH, PPL, 128><<<items, NT, 0, st>>>(a); break;
-    default: raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128)><<<items, NT, 0, st>>>(a); break;
+    case 64: raster_bwd_kernel<TW, TH, PPL, 64, REF><<<items, NT, 0, st>>>(a); break;
+    case 128: raster_bwd_kernel<TW, TH, PPL, 128, REF><<<items, NT, 0, st>>>(a); break;
+    default: raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128), REF><<<items, NT, 0, st>>>(a); break;
   }
   return cudaGetLastError();
+}
+template <int TW, int TH, int PPL>
+cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
+  return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, items, batch, st)
+                    : launch_bwd_mode<TW, TH, PPL, false>(a, items, batch, st);
 }
 
 }  // namespace
