@@ -669,6 +669,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     nbs = n2s;
     buf ^= 1;
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may outlive the block
   // Deterministic mode: list entries of this tile that no pixel reached keep
   // zero partial records.
   if (a.det) {
