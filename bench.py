@@ -361,7 +361,7 @@ def main():
     algo = {
         "raster_fwd": sum(40 * I[v] + 16 * P for v in range(nv)),
         "raster_bwd": sum(40 * I[v] + 32 * P + 56 * V[v] for v in range(nv)),
-        "tile_sort": sum(24 * I[v] for v in range(nv)),
+        "tile_sort": sum(16 * I[v] for v in range(nv)),  # two passes over packed 4-byte keys, read + write
         "project": 44 * args.n + sum((12 + 48 + 192) * V[v] for v in range(nv)),
         "adam": 28 * (10 + 48 + 1) * args.n + 8 * 10 * args.n,
     }
@@ -372,8 +372,8 @@ def main():
     # intersections), scaled to the launch by its intersections (the raster
     # and tile-sort traffic grows with them) or, for Adam, taken as is (it
     # sweeps the N parameters once per step).
-    traffic_coeff = {"raster_bwd": (38.71e6 + 0.035e6) / 6273269, "raster_fwd": (14.12e6 + 0.25e6) / 6273269,
-                     "tile_sort": (52.6e6 + 6.0e6 + 52.4e6 + 7.0e6) / 6273269}
+    traffic_coeff = {"raster_bwd": (37.742e6 + 0.023e6) / 6273269, "raster_fwd": (14.117e6 + 0.142e6) / 6273269,
+                     "tile_sort": (27.618e6 + 0.427e6 + 27.366e6 + 0.415e6) / 6273269}
     if dom in traffic_coeff:
         traffic = traffic_coeff[dom] * sum(I)
     elif dom == "adam":
