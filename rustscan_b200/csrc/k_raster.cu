@@ -347,7 +347,7 @@ __device__ __forceinline__ float warp_reduce_scatter16(float (&x)[16], int lane)
 struct BwdPair {
   uint32_t last0, last1;
   float2 T, K;          // transmittance, background term
-  float2 S0, S1, S2;    // colour accumulated behind the current Gaussian
+  float2 SV;            // dot(colour accumulated behind the current Gaussian, upstream colour gradient)
   float2 vr, vg, vb;    // upstream colour gradient
 };
 
@@ -372,7 +372,7 @@ __device__ __forceinline__ void load_bwd_pair(const RasterArgs& a, const ViewDes
   p.last1 = last[1];
   p.T = make_float2(T[0], T[1]);
   p.K = make_float2(K[0], K[1]);
-  p.S0 = p.S1 = p.S2 = f2(0.f);
+  p.SV = f2(0.f);
   p.vr = make_float2(g[0][0], g[1][0]);
   p.vg = make_float2(g[0][1], g[1][1]);
   p.vb = make_float2(g[0][2], g[1][2]);
@@ -439,11 +439,10 @@ __device__ __forceinline__ void bwd_pair_step(BwdPair& p, float2 npcy, uint32_t 
   const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
   const float2 cpv = fma2(f2(cp2), p.vb, fma2(f2(cp1), p.vg, mul2(f2(cp0), p.vr)));
   const float2 vis = mul2(am, Ti);
-  const float2 sv = fma2(p.S2, p.vb, fma2(p.S1, p.vg, mul2(p.S0, p.vr)));
-  const float2 va = fma2(Ti, cpv, neg2(mul2(add2(sv, p.K), ra)));
-  p.S0 = fma2(f2(cp0), vis, p.S0);
-  p.S1 = fma2(f2(cp1), vis, p.S1);
-  p.S2 = fma2(f2(cp2), vis, p.S2);
+  // The colour behind only enters through its dot product with the
+  // upstream gradient, which accumulates directly: sum vis_i * dot(c_i, v).
+  const float2 va = fma2(Ti, cpv, neg2(mul2(add2(p.SV, p.K), ra)));
+  p.SV = fma2(vis, cpv, p.SV);
   p.T = Ti;
   const bool gm0 = c0 && !sk0, gm1 = c1 && !sk1;
   const bool gg0 = gm0 && og.x <= 0.999f, gg1 = gm1 && og.y <= 0.999f;
