@@ -48,8 +48,12 @@ __global__ void __launch_bounds__(128) pair_bwd_kernel(PairArgs a) {
   const float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
   const uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
   float4* pair = slice(a.b.pair, a.b.Vcap * 6, v);
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < V; c += gridDim.x * blockDim.x) {
-    const uint32_t g = gid_of_c[c];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t g_next = c < V ? gid_of_c[c] : 0u;
+  for (; c < V; c += stride) {
+    const uint32_t g = g_next;
+    if (c + stride < V) g_next = gid_of_c[c + stride];  // the next row's id is in flight during this one
     const float2* t2 = reinterpret_cast<const float2*>(a.sp.transforms + (size_t)g * 10);
     const float2 t01 = t2[0], t23 = t2[1], t45 = t2[2], t67 = t2[3], t89 = t2[4];
     const float4 q0 = sgrad[(size_t)c * 3 + 0], q1 = sgrad[(size_t)c * 3 + 1], q2 = sgrad[(size_t)c * 3 + 2];

@@ -40,13 +40,14 @@ __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? l
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
-// Pass 1. Shared memory holds the five input planes (x, y, x^2, y^2, xy) of
-// the replicate-padded halo, then the horizontally blurred planes. Each
-// thread blurs two adjacent columns at once with paired FP32 arithmetic,
-// sliding one load per tap along the row (horizontal) or down the column
-// pair (vertical, two output rows per thread).
+// Pass 1. Shared memory holds the two input planes (x, y) of the
+// replicate-padded halo, then the five horizontally blurred planes (x, y,
+// x^2, y^2, xy; the products are formed as the row is read). Each thread
+// blurs two adjacent columns at once with paired FP32 arithmetic, sliding
+// one load per tap along the row (horizontal) or down the column pair
+// (vertical, two output rows per thread).
 struct SsimFwdSmem {
-  float p[5][HY][HX];
+  float p[2][HY][HX];
   float h[5][HY][LTX];
   float red[2][8];
 };
@@ -82,32 +83,42 @@ __global__ void __launch_bounds__(kLT) ssim_fwd_kernel(LossArgs a) {
       const int i = threadIdx.x + it * kLT;
       if (i < HX * HY) {
         const int hy = i / HX, hx = i % HX;
-        const float x = xs[it], y = ys[it];
-        S.p[0][hy][hx] = x;
-        S.p[1][hy][hx] = y;
-        S.p[2][hy][hx] = x * x;
-        S.p[3][hy][hx] = y * y;
-        S.p[4][hy][hx] = x * y;
+        S.p[0][hy][hx] = xs[it];
+        S.p[1][hy][hx] = ys[it];
       }
     }
   }
   __syncthreads();
-  // Horizontal pass: every halo row, output columns in pairs.
+  // Horizontal pass: every halo row, output columns in pairs; the five
+  // moment values of each input are formed once from x and y.
   for (int i = threadIdx.x; i < HY * (LTX / 2); i += blockDim.x) {
     const int hy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
+    const float* rx = &S.p[0][hy][ox];
+    const float* ry = &S.p[1][hy][ox];
+    float2 acc[5];
+    float prev[5];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      const float* row = &S.p[m][hy][ox];
-      float2 acc = f2(0.f);
-      float prev = row[0];
-#pragma unroll
-      for (int t = 0; t < WIN; ++t) {
-        const float next = row[t + 1];
-        acc = fma2(f2(a.k[t]), make_float2(prev, next), acc);
-        prev = next;
-      }
-      *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc;
+    for (int m = 0; m < 5; ++m) acc[m] = f2(0.f);
+    {
+      const float x = rx[0], y = ry[0];
+      prev[0] = x;
+      prev[1] = y;
+      prev[2] = x * x;
+      prev[3] = y * y;
+      prev[4] = x * y;
     }
+#pragma unroll
+    for (int t = 0; t < WIN; ++t) {
+      const float x = rx[t + 1], y = ry[t + 1];
+      const float next[5] = {x, y, x * x, y * y, x * y};
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        acc[m] = fma2(f2(a.k[t]), make_float2(prev[m], next[m]), acc[m]);
+        prev[m] = next[m];
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc[m];
   }
   __syncthreads();
   // Vertical pass and the SSIM map: a column pair times two rows per thread.

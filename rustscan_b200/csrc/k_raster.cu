@@ -135,12 +135,14 @@ __device__ __forceinline__ float2 sigma2(float t1, float t2, float2 dy, float cc
   return make_float2(blend_sigma_shared(t1, t2, dy.x, cc), blend_sigma_shared(t1, t2, dy.y, cc));
 }
 
-// blend_expf(-sigma) for both pixels. The argument is clamped to [-87, 0]
-// first, which leaves every sigma the contribution test can accept
-// (0 <= sigma <= log(255) + margin) unchanged, so for those the result is
-// bit-identical to blend_expf; for the others it stays finite.
+// blend_expf(-sigma) for both pixels, without its range clamps: for every
+// sigma the contribution test can accept (0 <= sigma <= log(255) + margin)
+// they change nothing, so there the result is bit-identical to blend_expf.
+// For a pixel outside that range the value is meaningless (possibly not
+// finite); every use of it is selected away by the pixel's contribution
+// flags, never multiplied in.
 __device__ __forceinline__ float2 blend_exp2(float2 sigma) {
-  const float xx = fmaxf(fminf(-sigma.x, 0.f), -87.f), xy = fmaxf(fminf(-sigma.y, 0.f), -87.f);
+  const float xx = -sigma.x, xy = -sigma.y;
   const float2 x = make_float2(xx, xy);
   const float2 t = make_float2(eadd(emul(xx, bexp::kLog2e), bexp::kMagic), eadd(emul(xy, bexp::kLog2e), bexp::kMagic));
   const float2 n = add2(t, f2(-bexp::kMagic));
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
   // Pixel q = 2k + h sits at row pyb + 4q and is half h of pair k.
   float2 T[NP], C0[NP], C1[NP], C2[NP], npcy[NP];
-  uint32_t last[PPL], nc[PPL], stop[PPL];
+  uint32_t last[PPL], nc[PPL];  // a pixel that saturates stops at its last contributor
   bool done[PPL];
   bool all_done = true;
 #pragma unroll
@@ -205,7 +207,6 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   for (int q = 0; q < PPL; ++q) {
     const uint32_t py = pyb + 4 * q;
     last[q] = nc[q] = 0;
-    stop[q] = s1;
     done[q] = !(px < vd.w && py < vd.h);
     all_done = all_done && done[q];
   }
@@ -260,18 +261,12 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
           if (c0) {
             last[2 * k] = b0 + j + 1;
             ++nc[2 * k];
-            if (T[k].x < 1e-4f) {
-              done[2 * k] = true;
-              stop[2 * k] = b0 + j + 1;
-            }
+            if (T[k].x < 1e-4f) done[2 * k] = true;
           }
           if (c1) {
             last[2 * k + 1] = b0 + j + 1;
             ++nc[2 * k + 1];
-            if (T[k].y < 1e-4f) {
-              done[2 * k + 1] = true;
-              stop[2 * k + 1] = b0 + j + 1;
-            }
+            if (T[k].y < 1e-4f) done[2 * k + 1] = true;
           }
         }
         all_done = true;
@@ -305,7 +300,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     slice(a.b.tfinal, a.b.Pcap, v)[pix] = Tq;
     slice(a.b.last, a.b.Pcap, v)[pix] = last[q];
     slice(a.b.ncontrib, a.b.Pcap, v)[pix] = nc[q];
-    slice(a.b.nvisit, a.b.Pcap, v)[pix] = stop[q] - s0;
+    slice(a.b.nvisit, a.b.Pcap, v)[pix] = (done[q] ? last[q] : s1) - s0;
   }
 }
 
