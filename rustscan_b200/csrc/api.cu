@@ -155,6 +155,9 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.ncontrib, nv * P) && dalloc(c, &b.nvisit, nv * P) && dalloc(c, &b.visible_c, nv * V) &&
             dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4) &&
             dalloc(c, &b.tile_hist, nv * T) && dalloc(c, &b.hitw, nv * I);
+  b.proj_parts_cap = (uint32_t)((N + 255) / 256);
+  ok = ok && dalloc(c, &b.vis_bits, nv * b.proj_parts_cap * 8) && dalloc(c, &b.blk_count, nv * b.proj_parts_cap) &&
+       dalloc(c, &b.blk_base, nv * b.proj_parts_cap);
   if (ok && cfg.deterministic)
     ok = dalloc(c, &b.sgrad_part, nv * I * 12) && dalloc(c, &b.inv_perm, nv * I);
   else {

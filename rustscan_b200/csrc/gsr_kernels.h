@@ -35,6 +35,10 @@ struct FwdBufs {
   uint32_t* nvisit;        // [P]
   uint8_t* visible_c;      // [V]
   uint8_t* hitw;           // [I] per list entry: forward warp blocks with a pixel that took it
+  uint32_t* vis_bits;      // projection: [views][proj_parts_cap * 8] visibility ballot words
+  uint32_t* blk_count;     // projection: [views][proj_parts_cap] visible per block of 256
+  uint32_t* blk_base;      // projection: [views][proj_parts_cap] exclusive scan of blk_count
+  uint32_t proj_parts_cap;
   float4* sgrad;           // [V][3] screen-space gradient sums (12 floats)
   float4* pair;            // [views][6][Vcap]: six float4 planes of projection adjoint records
   float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)

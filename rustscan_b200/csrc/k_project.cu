@@ -1,15 +1,19 @@
 // k_project.cu — projection, SH colour, tile counting and compaction.
 //
-// One thread per Gaussian evaluates every view of the launch: the
-// parameters are read once (the block stages its 256 x 40-byte transform
-// rows in shared memory with 128-bit loads, and its SH rows with coalesced
-// asynchronous copies that overlap the visibility phase), the thread projects the
-// Gaussian in every view (project_forward.wgsl:19-96, project_visible.wgsl:
-// 233-310) and the block compacts the visible ones in global-id order with a
-// decoupled look-back per view, all views' look-backs at once. The tiles each visible Gaussian touches are counted
-// afterwards by the warp-cooperative walk over the compact records. This replaces the
-// atomic compaction of project_forward.wgsl:94-96 (nondeterministic order)
-// and fuses the separate project_visible pass.
+// Three passes over every Gaussian and every view of the launch
+// (project_forward.wgsl:19-96, project_visible.wgsl:233-310):
+//  1. visibility: one thread per Gaussian projects it in every view and
+//     records warp ballot words and per-block visible counts (the block
+//     stages its 256 x 40-byte transform rows with 128-bit loads);
+//  2. one block per view scans the block counts;
+//  3. records: the visible Gaussians' compact indices follow in global-id
+//     order from the block base, the earlier warps' and lanes' bits; the
+//     projection is recomputed and the SH colour evaluated from the block's
+//     SH rows, staged in shared memory with coalesced asynchronous copies.
+// No block waits on another. The tiles each visible Gaussian touches are
+// counted afterwards by the warp-cooperative walk over the compact records.
+// This replaces the atomic compaction of project_forward.wgsl:94-96
+// (nondeterministic order) and fuses the separate project_visible pass.
 //
 // Projected record, three float4 per visible Gaussian:
 //   r0 = (x, y, conic_a, conic_b)
@@ -31,10 +35,11 @@ struct ProjectArgs {
   float cov_blur;
   int hp;
   FwdBufs b;
-  unsigned long long* states;  // [views][parts]
-  uint32_t parts;
-  LookbackCtl* ctl;
-  DevStatus* status;
+  uint32_t parts;       // blocks of kProjThreads Gaussians
+  uint32_t words;       // visibility words per view (parts * warps per block)
+  uint32_t* vis_bits;   // [views][words]
+  uint32_t* blk_count;  // [views][parts]
+  uint32_t* blk_base;   // [views][parts]
 };
 
 // The block's SH rows live in shared memory as FP32 with an odd row stride,
@@ -71,91 +76,147 @@ __device__ __forceinline__ void sh_rows_issue(const __nv_bfloat16* sh, uint32_t 
 }
 __device__ __forceinline__ void sh_rows_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <class SHT, int DEG>
-__global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
-  constexpr int kWarps = kProjThreads / 32;
-  extern __shared__ float s_sh[];  // [kProjThreads][ShRows<DEG>::kStride]
-  __shared__ float4 s_tr4[kProjThreads * 10 / 4];
-  __shared__ uint32_t s_mask[kMaxViews][kWarps];  // visibility ballots per view and warp
-  __shared__ uint32_t s_wpre[kMaxViews][kWarps];  // exclusive prefix over the warps
-  __shared__ uint32_t s_excl[kMaxViews];          // the partition's first compact index per view
-  __shared__ uint32_t s_part;
-  const uint32_t epoch = epoch_begin(a.ctl);
-  const uint32_t part = next_ticket(a.ctl, 0, &s_part);
-  const uint32_t n = a.sp.n;
-  const uint32_t nv = a.vs.n_views;
-  const uint32_t g0 = part * kProjThreads;
-  const uint32_t g = g0 + threadIdx.x;
-  const bool valid = g < n;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  float* s_tr = reinterpret_cast<float*>(s_tr4);
-  const uint32_t rows = g0 < n ? min(n - g0, (uint32_t)kProjThreads) : 0u;
-  // The SH rows are needed only in phase 2; their copy overlaps phase 1.
-  sh_rows_issue<DEG>(reinterpret_cast<const SHT*>(a.sp.sh), g0, rows, s_sh);
-  // Stage this block's transform rows: 256 * 10 floats, 16-byte aligned.
-  {
-    const float* src = a.sp.transforms + (size_t)g0 * 10;
-    if (rows == kProjThreads) {
-      const float4* src4 = reinterpret_cast<const float4*>(src);
-      for (int i = threadIdx.x; i < kProjThreads * 10 / 4; i += kProjThreads) s_tr4[i] = __ldg(src4 + i);
-    } else {
-      for (uint32_t i = threadIdx.x; i < rows * 10; i += kProjThreads) s_tr[i] = __ldg(src + i);
-    }
-  }
-  __syncthreads();
+// Stages the block's 256 transform rows (10 floats each, 16-byte aligned)
+// with 128-bit loads and reads this thread's parameters.
+struct GaussParams {
   V3<float> mean{0.f, 0.f, 0.f};
   V4<float> quat{1.f, 0.f, 0.f, 0.f};
   V3<float> ls{0.f, 0.f, 0.f};
   float raw = 0.f;
-  if (valid) {
-    const float* t = s_tr + threadIdx.x * 10;
-    mean = V3<float>{t[0], t[1], t[2]};
-    quat = V4<float>{t[3], t[4], t[5], t[6]};
-    ls = V3<float>{t[7], t[8], t[9]};
-    raw = __ldg(a.sp.raw_opac + g);
+};
+__device__ __forceinline__ GaussParams stage_params(const SplatsDev& sp, uint32_t g0, uint32_t rows, float4* s_tr4) {
+  float* s_tr = reinterpret_cast<float*>(s_tr4);
+  const float* src = sp.transforms + (size_t)g0 * 10;
+  if (rows == kProjThreads) {
+    const float4* src4 = reinterpret_cast<const float4*>(src);
+    for (int i = threadIdx.x; i < kProjThreads * 10 / 4; i += kProjThreads) s_tr4[i] = __ldg(src4 + i);
+  } else {
+    for (uint32_t i = threadIdx.x; i < rows * 10; i += kProjThreads) s_tr[i] = __ldg(src + i);
   }
+  __syncthreads();
+  GaussParams q;
+  if (threadIdx.x < rows) {
+    const float* t = s_tr + threadIdx.x * 10;
+    q.mean = V3<float>{t[0], t[1], t[2]};
+    q.quat = V4<float>{t[3], t[4], t[5], t[6]};
+    q.ls = V3<float>{t[7], t[8], t[9]};
+    q.raw = __ldg(sp.raw_opac + g0 + threadIdx.x);
+  }
+  return q;
+}
+
+// Pass 1: visibility of every Gaussian in every view. Each warp's ballot
+// word goes to vis_bits[view][warp], each block's count to
+// blk_count[view][block].
+__global__ void __launch_bounds__(kProjThreads) visibility_kernel(ProjectArgs a) {
+  constexpr int kWarps = kProjThreads / 32;
+  __shared__ float4 s_tr4[kProjThreads * 10 / 4];
+  __shared__ uint32_t s_cnt[kMaxViews][kWarps];
+  const uint32_t n = a.sp.n, nv = a.vs.n_views;
+  const uint32_t part = blockIdx.x;
+  const uint32_t g0 = part * kProjThreads;
+  const uint32_t rows = min(n - g0, (uint32_t)kProjThreads);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const GaussParams q = stage_params(a.sp, g0, rows, s_tr4);
+  const bool valid = threadIdx.x < rows;
   const TileShape ts{a.vs.tile_w, a.vs.tile_h};
-  // Phase 1: visibility in every view; the block's per-view counts are
-  // published together and the views' look-backs run in parallel (thread v
-  // resolves view v), so the block waits once instead of once per view.
   for (uint32_t v = 0; v < nv; ++v) {
     const ViewDesc& vd = a.vs.views[v];
     const Cam<float> cam = cam_from_desc<float>(vd);
     bool vis = false;
-    if (valid) vis = project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0).visible;
+    if (valid)
+      vis = project_gaussian(cam, q.mean, q.quat, q.ls, q.raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0)
+                .visible;
     const uint32_t m = __ballot_sync(0xffffffffu, vis);
-    if (lane == 0) s_mask[v][warp] = m;
+    if (lane == 0) {
+      a.vis_bits[(size_t)v * a.words + part * kWarps + warp] = m;
+      s_cnt[v][warp] = (uint32_t)__popc(m);
+    }
   }
   __syncthreads();
   if (threadIdx.x < nv) {
-    const uint32_t v = threadIdx.x;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) tot += s_cnt[threadIdx.x][w];
+    a.blk_count[(size_t)threadIdx.x * a.parts + part] = tot;
+  }
+}
+
+// Pass 2: per view (one block each), the exclusive scan of the block counts
+// in block order and the view's visible count.
+constexpr int kBlkScanThreads = 1024;
+__global__ void __launch_bounds__(kBlkScanThreads) block_scan_kernel(ProjectArgs a) {
+  __shared__ uint32_t s_scan[32];
+  __shared__ uint32_t s_carry;
+  const uint32_t v = blockIdx.x;
+  const uint32_t* cnt = a.blk_count + (size_t)v * a.parts;
+  uint32_t* base = a.blk_base + (size_t)v * a.parts;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t p0 = 0; p0 < a.parts; p0 += kBlkScanThreads) {
+    const uint32_t p = p0 + threadIdx.x;
+    const uint32_t x = p < a.parts ? cnt[p] : 0u;
+    uint32_t tot;
+    const uint32_t e = block_exclusive_scan(x, s_scan, &tot);
+    const uint32_t carry = s_carry;
+    if (p < a.parts) base[p] = carry + e;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry = carry + tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.b.vcount[v * 4 + 0] = s_carry;
+}
+
+// Pass 3: the visible Gaussians' records at their compact indices in
+// global-id order (block base + warps before + lanes before); the
+// projection is recomputed (the same expression on the same inputs), the SH
+// colour is evaluated from the block's staged SH rows.
+template <class SHT, int DEG>
+__global__ void __launch_bounds__(kProjThreads) records_kernel(ProjectArgs a) {
+  constexpr int kWarps = kProjThreads / 32;
+  extern __shared__ float s_sh[];  // [kProjThreads][ShRows<DEG>::kStride]
+  __shared__ float4 s_tr4[kProjThreads * 10 / 4];
+  __shared__ uint32_t s_mask[kMaxViews][kWarps];
+  __shared__ uint32_t s_wpre[kMaxViews][kWarps];
+  __shared__ uint32_t s_base[kMaxViews];
+  const uint32_t n = a.sp.n, nv = a.vs.n_views;
+  const uint32_t part = blockIdx.x;
+  const uint32_t g0 = part * kProjThreads;
+  const uint32_t g = g0 + threadIdx.x;
+  const uint32_t rows = min(n - g0, (uint32_t)kProjThreads);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  sh_rows_issue<DEG>(reinterpret_cast<const SHT*>(a.sp.sh), g0, rows, s_sh);
+  if (threadIdx.x < nv * kWarps) {
+    const uint32_t v = threadIdx.x / kWarps, w = threadIdx.x % kWarps;
+    s_mask[v][w] = a.vis_bits[(size_t)v * a.words + part * kWarps + w];
+  }
+  if (threadIdx.x < nv) s_base[threadIdx.x] = a.blk_base[(size_t)threadIdx.x * a.parts + part];
+  const GaussParams q = stage_params(a.sp, g0, rows, s_tr4);  // synchronises the block
+  if (threadIdx.x < nv) {
     uint32_t tot = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      s_wpre[v][w] = tot;
-      tot += (uint32_t)__popc(s_mask[v][w]);
+      s_wpre[threadIdx.x][w] = tot;
+      tot += (uint32_t)__popc(s_mask[threadIdx.x][w]);
     }
-    const uint32_t excl = lookback(a.states + (size_t)v * a.parts, 1, part, tot, epoch, a.status, kWaitCompact);
-    s_excl[v] = excl;
-    if (part == a.parts - 1) a.b.vcount[v * 4 + 0] = excl + tot;
   }
   sh_rows_wait();
   __syncthreads();
-  // Phase 2: the visible Gaussians' records at their compact indices (the
-  // projection is recomputed: the same expression on the same inputs).
+  const bool valid = threadIdx.x < rows;
+  const TileShape ts{a.vs.tile_w, a.vs.tile_h};
   const float* shg = s_sh + threadIdx.x * ShRows<DEG>::kStride;
   for (uint32_t v = 0; v < nv; ++v) {
     const uint32_t m = s_mask[v][warp];
     const bool vis = (m >> lane) & 1u;
-    const uint32_t c = s_excl[v] + s_wpre[v][warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    const uint32_t c = s_base[v] + s_wpre[v][warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
     if (valid) slice(a.b.c_of_gid, a.b.Ncap, v)[g] = vis ? (int32_t)c : -1;
     if (vis) {
       const ViewDesc& vd = a.vs.views[v];
       const Cam<float> cam = cam_from_desc<float>(vd);
       const Projected<float> p =
-          project_gaussian(cam, mean, quat, ls, raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
+          project_gaussian(cam, q.mean, q.quat, q.ls, q.raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
       auto coeff = [&](int k, int ch) { return shg[k * 3 + ch]; };
-      const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, mean), coeff);
+      const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, q.mean), coeff);
       float4* r = slice(a.b.rec, a.b.Vcap * 3, v) + (size_t)c * 3;
       r[0] = make_float4(p.mean2d.x, p.mean2d.y, p.conic.x, p.conic.y);
       r[1] = make_float4(p.conic.z, p.opacity, rgb.x, rgb.y);
@@ -165,15 +226,14 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(ProjectArgs a) {
       slice(a.b.depth_key, a.b.Vcap, v)[c] = __float_as_uint(p.depth);
     }
   }
-  epoch_end(a.ctl, epoch);
 }
 
 template <class SHT, int DEG>
 cudaError_t launch_deg(dim3 grid, cudaStream_t st, const ProjectArgs& a) {
   const size_t bytes = ShRows<DEG>::kBytes;
-  cudaError_t e = cudaFuncSetAttribute(project_kernel<SHT, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaError_t e = cudaFuncSetAttribute(records_kernel<SHT, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return e;
-  project_kernel<SHT, DEG><<<grid, kProjThreads, bytes, st>>>(a);
+  records_kernel<SHT, DEG><<<grid, kProjThreads, bytes, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -192,6 +252,7 @@ cudaError_t dispatch(int degree, dim3 grid, cudaStream_t st, const ProjectArgs& 
 
 cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blur, int fp64_conic, FwdBufs& b,
                            const Scratch& s, cudaStream_t st) {
+  (void)s;
   if (sp.n == 0) {
     // No Gaussians: every view has zero visible.
     for (uint32_t v = 0; v < vs.n_views; ++v) {
@@ -207,11 +268,14 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
   a.hp = fp64_conic;
   a.b = b;
   a.parts = (sp.n + kProjThreads - 1) / kProjThreads;
-  a.states = s.lb_states;
-  a.ctl = s.ctl;
-  a.status = s.status;
-  if ((uint64_t)a.parts * vs.n_views > s.lb_states_words) return cudaErrorInvalidValue;
-  dim3 grid(a.parts);
+  a.words = a.parts * (kProjThreads / 32);
+  if (a.parts > b.proj_parts_cap) return cudaErrorInvalidValue;
+  a.vis_bits = b.vis_bits;
+  a.blk_count = b.blk_count;
+  a.blk_base = b.blk_base;
+  visibility_kernel<<<a.parts, kProjThreads, 0, st>>>(a);
+  block_scan_kernel<<<vs.n_views, kBlkScanThreads, 0, st>>>(a);
+  const dim3 grid(a.parts);
   return sp.sh_bf16 ? dispatch<__nv_bfloat16>(sp.degree, grid, st, a) : dispatch<float>(sp.degree, grid, st, a);
 }
 
