@@ -394,29 +394,40 @@ struct BwdAcc {
   uint32_t n;         // contributing pixels
 };
 
-// One step of the reverse walk for both pixels of a pair: the contribution
-// decisions repeat the forward's bit for bit; the gradient follows
-// blend_step_grad (rasterize_backwards, exact adjoint), with the
-// transmittance recovered with a Newton-refined hardware reciprocal. Adds
-// the pair's terms into acc. With REF (the reference semantics) a pixel
-// whose transmittance fell to 1e-4 no longer counts as a contributor and
-// gets no gradient.
-template <bool REF>
-__device__ __forceinline__ void bwd_pair_step(BwdPair& p, float2 npcy, uint32_t s, float t1, float t2, float adx,
-                                              float bdx, float cb, const float4& A, const float4& B,
-                                              const float4& Cc, BwdAcc& acc) {
+// The first part of a reverse-walk step for both pixels of a pair: the
+// offsets and sigma, and whether each pixel can take the Gaussian at all
+// (it is before its last contributor and sigma is within the cut).
+struct PairPre {
+  float2 dy, sg;
+  bool l0, l1;
+};
+__device__ __forceinline__ PairPre bwd_pair_pre(const BwdPair& p, float2 npcy, uint32_t s, float t1, float t2,
+                                                const float4& A, const float4& B) {
+  PairPre q;
   const bool in0 = s < p.last0, in1 = s < p.last1;
-  if (!(in0 || in1)) return;
-  const float2 dy = make_float2(eadd(A.y, npcy.x), eadd(A.y, npcy.y));
-  const float2 sg = sigma2(t1, t2, dy, B.x);
-  const bool l0 = in0 && !(sg.x > B.y), l1 = in1 && !(sg.y > B.y);
-  if (!(l0 || l1)) return;
-  const float2 gs = blend_exp2(sg);
+  q.dy = make_float2(eadd(A.y, npcy.x), eadd(A.y, npcy.y));
+  q.sg = sigma2(t1, t2, q.dy, B.x);
+  q.l0 = in0 && !(q.sg.x > B.y);
+  q.l1 = in1 && !(q.sg.y > B.y);
+  return q;
+}
+
+// The rest of the step: the contribution decisions repeat the forward's bit
+// for bit; the gradient follows blend_step_grad (rasterize_backwards, exact
+// adjoint), with the transmittance recovered with a Newton-refined hardware
+// reciprocal. Adds the pair's terms into acc. Straight-line code: a pixel
+// that does not take the Gaussian contributes zeros and keeps its state.
+// With REF (the reference semantics) a pixel whose transmittance fell to
+// 1e-4 no longer counts as a contributor and gets no gradient.
+template <bool REF>
+__device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, float adx, float bdx, float cb,
+                                              const float4& B, const float2 cpv, BwdAcc& acc) {
+  const float2 dy = q.dy;
+  const float2 gs = blend_exp2(q.sg);
   const float2 og = mul2(f2(B.z), gs);
   const float ax = fminf(0.999f, og.x), ay = fminf(0.999f, og.y);
-  const bool c0 = l0 && sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
-  const bool c1 = l1 && sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
-  if (!(c0 || c1)) return;
+  const bool c0 = q.l0 && q.sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
+  const bool c1 = q.l1 && q.sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
   const bool sk0 = REF && p.T.x <= 1e-4f, sk1 = REF && p.T.y <= 1e-4f;
   const float2 al = make_float2(ax, ay);
   const float2 am = make_float2(c0 ? ax : 0.f, c1 ? ay : 0.f);
@@ -431,8 +442,6 @@ __device__ __forceinline__ void bwd_pair_step(BwdPair& p, float2 npcy, uint32_t 
 #endif
   ra = make_float2(c0 ? ra.x : 1.f, c1 ? ra.y : 1.f);
   const float2 Ti = mul2(p.T, ra);
-  const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
-  const float2 cpv = fma2(f2(cp2), p.vb, fma2(f2(cp1), p.vg, mul2(f2(cp0), p.vr)));
   const float2 vis = mul2(am, Ti);
   // The colour behind only enters through its dot product with the
   // upstream gradient, which accumulates directly: sum vis_i * dot(c_i, v).
@@ -601,10 +610,35 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
         acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.op = f2(0.f);
         acc.ax = acc.ay = 0.f;
         acc.n = 0u;
+        const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
+        PairPre pre[NP];
+        uint32_t need = 0;  // pairs with a pixel that can take the Gaussian, over the warp
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
           const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
-          bwd_pair_step<REF>(pp[k], npcy, s, t1, t2, adx, bdx, cb, A, B, Cc, acc);
+          pre[k] = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
+          if (__any_sync(0xffffffffu, pre[k].l0 || pre[k].l1)) need |= 1u << k;
+        }
+        // Pairs needed by the warp run as one straight-line block, so that
+        // their independent instruction chains interleave.
+        auto rest = [&](int k) {
+          const float2 cpv =
+              fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
+          bwd_pair_rest<REF>(pp[k], pre[k], adx, bdx, cb, B, cpv, acc);
+        };
+        if constexpr (NP == 2) {
+          if (need == 3u) {
+            rest(0);
+            rest(1);
+          } else if (need == 1u) {
+            rest(0);
+          } else if (need == 2u) {
+            rest(1);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NP; ++k)
+            if (need & (1u << k)) rest(k);
         }
         const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
         float x[16];
