@@ -161,6 +161,15 @@ __device__ __forceinline__ float2 blend_exp2(float2 sigma) {
   return make_float2(__uint_as_float(__float_as_uint(p.x) + ex), __uint_as_float(__float_as_uint(p.y) + ey));
 }
 
+// Per-entry terms of a forward step for one pixel pair.
+struct FwdPre {
+  float2 sg;       // sigma of both pixels
+  float opac;
+  float ax, ay;    // alpha of both pixels
+  bool l0, l1;     // within the cut
+  bool c0, c1;     // contributes (before the pixel-state gate)
+};
+
 template <int TW, int TH, int PPL, int BATCH>
 __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) {
   static_assert(PPL % 2 == 0, "pixels per lane come in pairs");
@@ -227,30 +236,51 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     __syncthreads();
     if (!__all_sync(0xffffffffu, all_done)) {
       const int cnt = build_list(s_mask, nb, warp, lane, s_list[warp]);
-      for (int e = 0; e < cnt; ++e) {
-        const uint32_t j = s_list[warp][e];
-        const float4 A = s_a[j];
-        const float4 B = s_b[j];
-        const float dx = esub(A.x, pcx);
-        const float t1 = emul(emul(A.z, dx), dx);
-        const float t2 = emul(A.w, dx);
+      // Entries go two at a time: the sigma, cut test, exponential and
+      // contribution test of both (independent of the pixel state) form one
+      // straight-line block whose chains interleave; the blends then apply
+      // in list order, the second gated by the pixel state the first left.
+      for (int e = 0; e < cnt; e += 2) {
+        const bool two = e + 1 < cnt;  // warp-uniform
+        const uint32_t jj[2] = {s_list[warp][e], two ? s_list[warp][e + 1] : s_list[warp][e]};
+        FwdPre pre[2][NP];
+        uint32_t need = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-          const bool d0 = done[2 * k], d1 = done[2 * k + 1];
-          if (d0 && d1) continue;
-          const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
-          const float2 sg = sigma2(t1, t2, dy, B.x);
-          const bool l0 = !d0 && !(sg.x > B.y), l1 = !d1 && !(sg.y > B.y);
-          if (!(l0 || l1)) continue;
-          const float2 og = mul2(f2(B.z), blend_exp2(sg));
-          const float ax = fminf(0.999f, og.x), ay = fminf(0.999f, og.y);
-          // blend_alpha_of: sigma >= 0 and alpha >= 1/255.
-          const bool c0 = l0 && sg.x >= 0.f && ax >= (float)(1.0 / 255.0);
-          const bool c1 = l1 && sg.y >= 0.f && ay >= (float)(1.0 / 255.0);
-          if (!(c0 || c1)) continue;
-          // A pixel that does not take this Gaussian blends with alpha 0,
-          // which leaves its colour and transmittance bit for bit unchanged.
-          const float2 am = make_float2(c0 ? ax : 0.f, c1 ? ay : 0.f);
+        for (int u = 0; u < 2; ++u) {
+          const float4 A = s_a[jj[u]];
+          const float4 B = s_b[jj[u]];
+          const float dx = esub(A.x, pcx);
+          const float t1 = emul(emul(A.z, dx), dx);
+          const float t2 = emul(A.w, dx);
+#pragma unroll
+          for (int k = 0; k < NP; ++k) {
+            FwdPre& q = pre[u][k];
+            const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
+            q.sg = sigma2(t1, t2, dy, B.x);
+            q.l0 = !(q.sg.x > B.y);
+            q.l1 = !(q.sg.y > B.y);
+            q.opac = B.z;
+            if (__any_sync(0xffffffffu, (q.l0 && !done[2 * k]) || (q.l1 && !done[2 * k + 1])) && (u == 0 || two))
+              need |= 1u << (u * NP + k);
+          }
+        }
+        // blend_alpha_of (sigma >= 0 and alpha >= 1/255) and the blend of
+        // entry u, pair k. A pixel that does not take the Gaussian blends
+        // with alpha 0, which leaves its colour and transmittance bit for bit
+        // unchanged.
+        auto alpha = [&](FwdPre& q) {
+          const float2 og = mul2(f2(q.opac), blend_exp2(q.sg));
+          q.ax = fminf(0.999f, og.x);
+          q.ay = fminf(0.999f, og.y);
+          q.c0 = q.l0 && q.sg.x >= 0.f && q.ax >= (float)(1.0 / 255.0);
+          q.c1 = q.l1 && q.sg.y >= 0.f && q.ay >= (float)(1.0 / 255.0);
+        };
+        auto blend = [&](int u, int k) {
+          const FwdPre& q = pre[u][k];
+          const bool c0 = q.c0 && !done[2 * k], c1 = q.c1 && !done[2 * k + 1];
+          if (!(c0 || c1)) return;
+          const uint32_t j = jj[u];
+          const float2 am = make_float2(c0 ? q.ax : 0.f, c1 ? q.ay : 0.f);
           const float4 Cc = s_c[j];
           const float2 w = mul2(am, T[k]);
           C0[k] = fma2(f2(Cc.x), w, C0[k]);  // blend_accum; Cc was clamped at staging
@@ -268,6 +298,19 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
             ++nc[2 * k + 1];
             if (T[k].y < 1e-4f) done[2 * k + 1] = true;
           }
+        };
+        static_assert(NP == 1, "the forward runs one pixel pair per lane");
+        if (need == 3u) {
+          alpha(pre[0][0]);
+          alpha(pre[1][0]);
+          blend(0, 0);
+          blend(1, 0);
+        } else if (need == 1u) {
+          alpha(pre[0][0]);
+          blend(0, 0);
+        } else if (need == 2u) {
+          alpha(pre[1][0]);
+          blend(1, 0);
         }
         all_done = true;
 #pragma unroll
