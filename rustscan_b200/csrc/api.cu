@@ -305,7 +305,7 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   b.pack_bits = (tile_counts && !c->cfg.deterministic && tbits + ibits <= 32) ? (uint32_t)ibits : 0u;
   if (tile_counts) {
     GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, st));
-    GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, st));
+    GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, tbits, st));
   } else {
     GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));
   }

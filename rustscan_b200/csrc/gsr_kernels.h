@@ -99,6 +99,16 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
 // vals_out == nullptr sorts the keys alone. The digits are `bits` bits
 // from bit shift0 up. The result lands in keys_out/vals_out; tmp buffers
 // are clobbered.
+// Radix passes and digit width for a sort over `bits` key bits.
+inline int sort_passes(int bits) {
+  const int p = (bits + 7) / 8;
+  return p < 1 ? 1 : (p > 4 ? 4 : p);
+}
+inline int sort_digit_bits(int bits) {
+  const int p = sort_passes(bits);
+  const int d = (bits + p - 1) / p;
+  return d < 1 ? 1 : (d > 8 ? 8 : d);
+}
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
                              uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
@@ -131,7 +141,9 @@ cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int det
 // ranges kernel. For views of at most kHistMaxTiles tiles.
 constexpr uint32_t kHistMaxTiles = 8192;
 cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
-cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
+// Tile ranges and the tile sort's digit histograms (digits of
+// sort_digit_bits(bits_for(max tiles)) bits) from emission's tile counts.
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, cudaStream_t st);
 // Packed mode only: intersections [0, n) of a view as separate tile ids and
 // compact indices.
 cudaError_t launch_unpack_isects(const FwdBufs& b, uint32_t view, uint32_t n, uint32_t* tiles, uint32_t* vals,

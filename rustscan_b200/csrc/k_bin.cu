@@ -187,10 +187,11 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
 
 // From the per-tile counts of one view: the tile ranges
 // (get_tile_offsets.wgsl:11-30 — [start, end) per tile, 0,0 when empty) and
-// the digit histograms of the tile sort's two passes (low and high byte of
-// the tile id), in the sort's histogram layout.
+// the digit histograms of the tile sort's (at most two) passes over the
+// tile id's digits, in the sort's histogram layout.
 constexpr int kHistThreads = 1024;
-__global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist) {
+__global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist,
+                                                                         uint32_t dbits) {
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_h[2][256];
   const uint32_t v = blockIdx.x;
@@ -217,8 +218,9 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
       ranges[2 * t] = loc[i] ? run : 0u;
       ranges[2 * t + 1] = loc[i] ? run + loc[i] : 0u;
       if (loc[i]) {
-        atomicAdd(&s_h[0][t & 255u], loc[i]);
-        atomicAdd(&s_h[1][(t >> 8) & 255u], loc[i]);
+        const uint32_t dm = (1u << dbits) - 1u;
+        atomicAdd(&s_h[0][t & dm], loc[i]);
+        atomicAdd(&s_h[1][(t >> dbits) & dm], loc[i]);
       }
     }
     run += loc[i];
@@ -351,9 +353,9 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
   return cudaGetLastError();
 }
 
-cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st) {
-  if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
-  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist);
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, cudaStream_t st) {
+  if (vs.max_tiles > kHistMaxTiles || sort_passes(tile_bits) > 2) return cudaErrorInvalidValue;
+  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits));
   return cudaGetLastError();
 }
 

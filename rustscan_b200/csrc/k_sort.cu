@@ -12,8 +12,9 @@
 //    back across partitions for their global offsets, then scatter through
 //    shared memory so that every digit's run is written contiguously;
 //  - scans are single-pass with the same look-back.
-// Keys are u32; `bits` limits the passes (8 bits each, starting at bit
-// shift0). Stability (ties in input order) is what the reference's index
+// Keys are u32; `bits` (from bit shift0) set the passes: ceil(bits / 8)
+// passes of equal digits of at most 8 bits (12 bits: two 6-bit passes, whose
+// 64 digit runs per partition are written in longer stretches than 256). Stability (ties in input order) is what the reference's index
 // tie-break provides (radix_sort.wgsl:21-26). Without values, the keys are
 // sorted alone (the binning packs tile id and compact index into one key
 // when both fit in 32 bits).
@@ -39,7 +40,7 @@ __device__ __forceinline__ uint32_t seg_count(const uint32_t* counts, uint32_t s
 __global__ void __launch_bounds__(256) sort_hist_kernel(const uint32_t* keys, uint64_t seg_stride,
                                                         const uint32_t* counts, uint32_t count_stride,
                                                         uint32_t n_host, uint64_t cap, int passes, uint32_t shift0,
-                                                        uint32_t* hist) {
+                                                        uint32_t dbits, uint32_t* hist) {
   __shared__ uint32_t h[4][256];
   for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(const uint32_t* keys, ui
   const uint32_t* k = keys + (size_t)seg * seg_stride;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t key = k[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(key >> (shift0 + 8 * p)) & 255u], 1u);
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(key >> (shift0 + dbits * p)) & ((1u << dbits) - 1u)], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
@@ -76,6 +77,7 @@ struct SortPassArgs {
   uint32_t n_host;
   uint64_t cap;
   uint32_t shift;
+  uint32_t dmask;  // digit mask: (1 << digit bits) - 1, at most 255
   uint32_t pass;
   const uint32_t* base;  // [seg][4][256]
   unsigned long long* states;
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
     for (int i = 0; i < kSortItems; ++i) {
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       const bool ok = idx < n;
-      const uint32_t d = ok ? ((key[i] >> a.shift) & 255u) : (256u + lane);
+      const uint32_t d = ok ? ((key[i] >> a.shift) & a.dmask) : (256u + lane);
       const uint32_t peers = __match_any_sync(0xffffffffu, d);
       const uint32_t below = peers & lt_mask;
       uint32_t b = 0;
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
     for (int i = 0; i < kSortItems; ++i) {
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       if (idx < n) {
-        const uint32_t dd = (key[i] >> a.shift) & 255u;
+        const uint32_t dd = (key[i] >> a.shift) & a.dmask;
         const uint32_t pos = s_dstart[dd] + s_whist[warp][dd] + lrank[i];
         s_keys[pos] = key[i];
         if (KV) s_vals[pos] = val[i];
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a)
     const uint32_t nvalid = min((uint32_t)kSortTile, n - tile0);
     for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
       const uint32_t k = s_keys[j];
-      const uint32_t dst = s_gbase[(k >> a.shift) & 255u] + j;
+      const uint32_t dst = s_gbase[(k >> a.shift) & a.dmask] + j;
       kout[dst] = k;
       if (KV) vout[dst] = s_vals[j];
     }
@@ -275,9 +277,8 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
   if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
   if (shift0 >= 32 || (keys_in == nullptr)) return cudaErrorInvalidValue;
   const bool kv = vals_out != nullptr;
-  int passes = (bits + 7) / 8;
-  if (passes < 1) passes = 1;
-  if (passes > 4) passes = 4;
+  const int dbits = sort_digit_bits(bits);
+  const int passes = sort_passes(bits);
   const uint32_t parts_cap = (uint32_t)((cap_per_segment + kSortTile - 1) / kSortTile);
   if ((uint64_t)parts_cap * 256 * segments > s.lb_states_words) return cudaErrorInvalidValue;
   if (!hist_ready) {
@@ -285,7 +286,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     if (e != cudaSuccess) return e;
     dim3 grid(persistent_blocks(s.num_sms, segments, 4), segments);
     sort_hist_kernel<<<grid, 256, 0, st>>>(keys_in, seg_stride, counts, count_stride, n_host, cap_per_segment, passes,
-                                           shift0, s.hist);
+                                           shift0, (uint32_t)dbits, s.hist);
   }
   sort_hist_scan_kernel<<<dim3(passes, segments), 256, 0, st>>>(s.hist, s.hist_base);
   // Ping-pong so that the last pass writes keys_out/vals_out.
@@ -305,7 +306,8 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.count_stride = count_stride;
     a.n_host = n_host;
     a.cap = cap_per_segment;
-    a.shift = shift0 + 8 * p;
+    a.shift = shift0 + dbits * p;
+    a.dmask = (1u << dbits) - 1u;
     a.pass = p;
     a.base = s.hist_base;
     a.states = s.lb_states;
