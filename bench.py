@@ -402,15 +402,19 @@ def main():
     # ---- end to end through the public API with host buffers -------------------
     host_t = torch.empty(targets.shape, dtype=torch.float32, pin_memory=True)
     host_t.copy_(targets.cpu())
-    dev_t = torch.empty_like(targets)
     host_loss = torch.empty(nv, dtype=torch.float32, pin_memory=True)
+    e2e_warm = 1
 
     def e2e_step(it):
-        dev_t.copy_(host_t, non_blocking=True)
-        loss = trainer.train_step(cams, dev_t, it)
+        # Each timed step's targets cross PCIe once: the first timed step
+        # copies its own, every other one was prefetched by the step before
+        # it (inside the timed region); the warm-up and the last timed step
+        # prefetch nothing.
+        nxt = host_t if e2e_warm < it < e2e_warm + args.steps else None
+        loss = trainer.train_step_host(cams, host_t, it, next_host_targets=nxt)
         host_loss.copy_(loss, non_blocking=True)
 
-    ms_e2e = time_steps(e2e_step, args.steps, 1, world) / args.steps
+    ms_e2e = time_steps(e2e_step, args.steps, e2e_warm, world) / args.steps
     e2e = {"value": ms_e2e / nv, "unit": UNIT, "h2d_bytes_per_step": int(host_t.numel() * 4),
            "d2h_bytes_per_step": int(nv * 4)}
 

@@ -487,6 +487,8 @@ class Trainer:
         self.densify = torch.zeros((9, splats.num_splats()), dtype=torch.float32, device="cuda")
         self.loss = None
         self._cams = None
+        self._h2d = None  # host-target pipeline: device targets, staging buffer, copy stream, events
+        self._prefetched = None
 
     def train_step(self, cameras, targets: torch.Tensor, iteration: int):
         cams = list(cameras)
@@ -508,3 +510,46 @@ class Trainer:
             C.byref(st), self._arr, len(cams), _ptr(targets), C.byref(p), _ptr(self.densify), _ptr(self.loss),
             int(self.use_graph), _stream()))
         return self.loss
+
+    def train_step_host(self, cameras, host_targets: torch.Tensor, iteration: int, next_host_targets=None):
+        """One step whose targets live in pinned host memory.
+
+        The targets are copied to the device (or, when the previous call was
+        given them as its next_host_targets, taken from the staging buffer
+        that call filled on a side stream while its step ran), the step runs
+        on the current stream, and next_host_targets, if given, start copying
+        into the staging buffer so that the copy overlaps this step. The
+        device buffer the step reads stays the same across calls, so a
+        captured step graph is replayed, not captured again. Returns the
+        per-view losses (device)."""
+        if not host_targets.is_pinned():
+            raise ValueError("host targets must be in pinned memory")
+        main = torch.cuda.current_stream()
+        h = self._h2d
+        if h is None or h["dev"].shape != host_targets.shape:
+            h = self._h2d = {
+                "dev": torch.empty(host_targets.shape, dtype=host_targets.dtype, device="cuda"),
+                "stage": torch.empty(host_targets.shape, dtype=host_targets.dtype, device="cuda"),
+                "stream": torch.cuda.Stream(),
+                "ready": torch.cuda.Event(),
+                "free": torch.cuda.Event(),
+            }
+            self._prefetched = None
+        if self._prefetched is not None and self._prefetched is host_targets:
+            main.wait_event(h["ready"])
+            h["dev"].copy_(h["stage"], non_blocking=True)
+        else:
+            h["dev"].copy_(host_targets, non_blocking=True)
+        h["free"].record(main)  # the staging buffer has been read
+        loss = self.train_step(cameras, h["dev"], iteration)
+        self._prefetched = None
+        if next_host_targets is not None:
+            if not next_host_targets.is_pinned() or next_host_targets.shape != host_targets.shape:
+                raise ValueError("next host targets must be pinned and of the same shape")
+            cs = h["stream"]
+            cs.wait_event(h["free"])
+            with torch.cuda.stream(cs):
+                h["stage"].copy_(next_host_targets, non_blocking=True)
+            h["ready"].record(cs)
+            self._prefetched = next_host_targets
+        return loss

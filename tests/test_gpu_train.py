@@ -124,3 +124,36 @@ def test_train_step_loss_and_statistics_vs_oracle(gsr_ctx_factory):
         b = f.backward(vp, mode=0)
         O.densify(b["v_transforms"], b["stats"], b["v_sh"], f.visible, acc)
     assert_grad_close(tr.densify.cpu().numpy(), acc, rtol=1e-3, what="densification statistics")
+
+
+def test_host_target_pipeline_equals_device_targets(gsr_ctx_factory):
+    """train_step_host (targets in pinned host memory, the next step's copy
+    prefetched on a side stream while the current step runs) is bit-identical
+    to train_step on device targets, and changing targets between calls takes
+    effect (the prefetched buffer is the one the step reads)."""
+    import torch
+
+    from rustscan_b200 import LearningRates, Trainer
+
+    sc, targets = _scene_pair(seed=90)
+    nv = len(sc.cameras)
+    flat = np.concatenate([t.reshape(-1) for t in targets]).astype(np.float32)
+    other = np.clip(flat[::-1] * 0.5 + 0.25, 0, 1).astype(np.float32)
+    seq = [flat, flat, other, flat, other, other]
+    hosts = [torch.from_numpy(x).pin_memory() for x in seq]
+    lrs = LearningRates()
+    ctx_a = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48, deterministic=True)
+    ctx_b = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48, deterministic=True)
+    sa, sb = _dev(sc), _dev(sc)
+    ta = Trainer(ctx_a, sa, lrs, use_graph=True, total_iterations=100)
+    tb = Trainer(ctx_b, sb, lrs, use_graph=True, total_iterations=100)
+    for it in range(1, len(seq) + 1):
+        nxt = hosts[it] if it < len(seq) else None
+        la = ta.train_step_host(sc.cameras, hosts[it - 1], it, next_host_targets=nxt).clone()
+        lb = tb.train_step(sc.cameras, torch.as_tensor(seq[it - 1], device="cuda"), it).clone()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(la.cpu().numpy(), lb.cpu().numpy())
+    np.testing.assert_array_equal(sa.transforms.cpu().numpy(), sb.transforms.cpu().numpy())
+    np.testing.assert_array_equal(sa.sh_coeffs.cpu().numpy(), sb.sh_coeffs.cpu().numpy())
+    with pytest.raises(ValueError):
+        ta.train_step_host(sc.cameras, torch.from_numpy(flat), 99)
