@@ -197,6 +197,29 @@ GSR_API gsr_status gsr_render_backward(gsr_ctx* ctx, const gsr_splats* splats, c
  * `bytes` is the destination size; the call fails if it is too small. */
 GSR_API gsr_status gsr_export(gsr_ctx* ctx, uint32_t view, int32_t what, void* dst, uint64_t bytes, void* stream);
 
+/* ---- training targets from 8-bit frames ----------------------------------- */
+/* One decoded colour frame: width x height RGB bytes (row-major, 3 bytes a
+ * pixel) at byte `offset` of a frame buffer. */
+typedef struct gsr_frame {
+  uint64_t offset;
+  uint32_t width, height;
+} gsr_frame;
+
+/* Converts n_views (at most 64) decoded 8-bit RGB frames into the targets
+ * gsr_loss and gsr_train_step read: per view [H,W,3] f32 with W, H from
+ * cams[v], views packed one after another. Replaces the host-side
+ * resize_rgb_u8_to_f32 (RustGS/src/training/data/frame_targets.rs:44-62)
+ * before the per-step f32 upload (engine/trainer.rs:94-107, 265-268): the
+ * caller uploads the bytes (a quarter of the f32 volume) and the conversion
+ * runs on the device. A frame of the camera's size maps each byte b to
+ * b / 255; any other size is box-averaged with the reference's bounds
+ * (output (x, y) averages source columns [x*sw/dw, max((x+1)*sw/dw,
+ * x*sw/dw + 1)) and the same rows, clamped to the frame) and summation
+ * order, so the results equal the reference's floats. frames and targets
+ * are device pointers; desc and cams host arrays. Enqueue only. */
+GSR_API gsr_status gsr_frames_to_targets(gsr_ctx* ctx, const uint8_t* frames, const gsr_frame* desc,
+                                         const gsr_camera* cams, uint32_t n_views, float* targets, void* stream);
+
 /* ---- loss (RustGS/src/training/engine/loss.rs:112-142) -------------------- */
 /* l1_w * mean|pred - target| + ssim_w * (1 - mean SSIM) with an 11-tap
  * sigma-1.5 Gaussian window, replicate padding and C1 = 0.01^2,

@@ -570,6 +570,36 @@ struct orc_fwd_f64 {
 
 #define ORC_EXPORT __attribute__((visibility("default")))
 
+// ---- frame targets (training/data/frame_targets.rs) ----
+// resize_rgb_u8_to_f32 (:44-62): each byte / 255; a frame of another size is
+// then box-averaged by resize_rgb (:1-42), rows and columns in order.
+ORC_EXPORT void orc_frame_to_target(const uint8_t* src, uint32_t sw, uint32_t sh, uint32_t dw, uint32_t dh,
+                                    float* dst) {
+  if (sw == dw && sh == dh) {
+    for (uint64_t i = 0; i < (uint64_t)sw * sh * 3; ++i) dst[i] = (float)src[i] / 255.0f;
+    return;
+  }
+  for (uint64_t dy = 0; dy < dh; ++dy) {
+    const uint64_t sy0 = dy * sh / dh;
+    const uint64_t sy1 = std::min(std::max((dy + 1) * sh / dh, sy0 + 1), (uint64_t)sh);
+    for (uint64_t dx = 0; dx < dw; ++dx) {
+      const uint64_t sx0 = dx * sw / dw;
+      const uint64_t sx1 = std::min(std::max((dx + 1) * sw / dw, sx0 + 1), (uint64_t)sw);
+      float acc[3] = {0.f, 0.f, 0.f};
+      uint64_t count = 0;
+      for (uint64_t sy = sy0; sy < sy1; ++sy)
+        for (uint64_t sx = sx0; sx < sx1; ++sx) {
+          const uint8_t* q = src + (sy * sw + sx) * 3;
+          for (int c = 0; c < 3; ++c) acc[c] = acc[c] + (float)q[c] / 255.0f;
+          ++count;
+        }
+      const float inv = 1.0f / (float)(count > 0 ? count : 1);
+      float* o = dst + (dy * dw + dx) * 3;
+      for (int c = 0; c < 3; ++c) o[c] = acc[c] * inv;
+    }
+  }
+}
+
 // ---- primitives (gpu_primitives/*) ----
 // Inclusive scan (prefix_sum.rs:53-136).
 ORC_EXPORT void orc_prefix_sum_u32(const uint32_t* in, uint32_t* out, uint64_t n) {

@@ -35,6 +35,8 @@ def lib():
             build()
         L = C.CDLL(_LIB_PATH)
         L.orc_prefix_sum_u32.argtypes = [u32p, u32p, C.c_uint64]
+        L.orc_frame_to_target.argtypes = [C.POINTER(C.c_uint8), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          f32p]
         L.orc_sort_pairs_u32.argtypes = [u32p, u32p, u32p, u32p, C.c_uint64]
         L.orc_expf.argtypes = [C.c_float]
         L.orc_expf.restype = C.c_float
@@ -171,6 +173,18 @@ class Forward:
         if getattr(self, "_h", None):
             getattr(lib(), f"orc_free_{self.suf}")(self._h)
             self._h = None
+
+
+def frame_to_target(frame_u8, width, height, dst_width, dst_height):
+    """resize_rgb_u8_to_f32 (frame_targets.rs:44-62): [height, width, 3] bytes
+    to a [dst_height, dst_width, 3] f32 target."""
+    src = np.ascontiguousarray(frame_u8, dtype=np.uint8).reshape(-1)
+    if src.size != width * height * 3:
+        raise ValueError("frame size does not match width x height x 3")
+    out = np.zeros((dst_height, dst_width, 3), np.float32)
+    lib().orc_frame_to_target(src.ctypes.data_as(C.POINTER(C.c_uint8)), width, height, dst_width, dst_height,
+                              _p(out, f32p))
+    return out
 
 
 def loss(pred, target, l1_weight=0.8, ssim_weight=0.2, f64=False):

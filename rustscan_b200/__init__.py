@@ -279,6 +279,39 @@ class Context:
         return loss, vp
 
 
+def frame_array(descs):
+    """(offset, width, height) triples as a gsr_frame array."""
+    arr = (_lib.gsr_frame * len(descs))()
+    for i, (off, w, h) in enumerate(descs):
+        arr[i].offset, arr[i].width, arr[i].height = int(off), int(w), int(h)
+    return arr
+
+
+def _frames_to_targets(ctx, frames: torch.Tensor, descs, cameras, out: torch.Tensor | None = None):
+    cams = list(cameras)
+    if len(descs) != len(cams):
+        raise ValueError("one frame per camera")
+    n = sum(c.width * c.height * 3 for c in cams)
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+    if out.numel() < n or not out.is_contiguous() or out.dtype != torch.float32:
+        raise ValueError("target buffer too small or not contiguous f32")
+    if frames.dtype != torch.uint8 or not frames.is_cuda or not frames.is_contiguous():
+        raise ValueError("frames must be a contiguous uint8 device tensor")
+    ctx._check(ctx._lib.gsr_frames_to_targets(ctx._h, _ptr(frames), frame_array(descs), camera_array(cams),
+                                              len(cams), _ptr(out), _stream()))
+    return out
+
+
+Context.frames_to_targets = _frames_to_targets
+Context.frames_to_targets.__doc__ = (
+    """Training targets from decoded 8-bit RGB frames on the device
+    (gsr_frames_to_targets): frames is a uint8 device buffer, descs the
+    (byte offset, width, height) of each view's frame; returns (or fills
+    `out`) the packed per-view [H,W,3] f32 targets at the cameras'
+    resolutions.""")
+
+
 def prefix_sum_u32(x: torch.Tensor, ctx: Context | None = None) -> torch.Tensor:
     ctx = ctx or Context(max_splats=max(x.numel(), 1))
     return ctx.prefix_sum_u32(x)
@@ -489,6 +522,8 @@ class Trainer:
         self._cams = None
         self._h2d = None  # host-target pipeline: device targets, staging buffer, copy stream, events
         self._prefetched = None
+        self._frames = None  # 8-bit frame pipeline: the same, with a byte staging buffer
+        self._frames_prefetched = None
 
     def train_step(self, cameras, targets: torch.Tensor, iteration: int):
         cams = list(cameras)
@@ -510,6 +545,69 @@ class Trainer:
             C.byref(st), self._arr, len(cams), _ptr(targets), C.byref(p), _ptr(self.densify), _ptr(self.loss),
             int(self.use_graph), _stream()))
         return self.loss
+
+    def train_step_frames(self, cameras, frames, iteration: int, next_frames=None):
+        """One step whose targets are decoded 8-bit RGB frames in pinned host
+        memory (frames: one [H,W,3] uint8 tensor per camera, e.g.
+        frames.DecodedFrame.rgb).
+
+        The bytes (a quarter of the f32 volume) cross to the device, or were
+        already copied there on a side stream during the previous call when
+        that call was given them as next_frames; gsr_frames_to_targets then
+        converts them into the step's target buffer (resizing frames whose
+        size differs from the camera's), and the step runs on the current
+        stream. next_frames, if given, start copying while this step runs.
+        Returns the per-view losses (device)."""
+        cams = list(cameras)
+        frames = list(frames)
+        if len(frames) != len(cams):
+            raise ValueError("one frame per camera")
+        for f in frames:
+            if f.dtype != torch.uint8 or f.dim() != 3 or f.shape[2] != 3 or not f.is_pinned():
+                raise ValueError("frames must be pinned [H,W,3] uint8 tensors")
+        sizes = [f.numel() for f in frames]
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).tolist()
+        descs = [(o, f.shape[1], f.shape[0]) for o, f in zip(offs, frames)]
+        n_t = sum(c.width * c.height * 3 for c in cams)
+        main = torch.cuda.current_stream()
+        h = self._frames
+        if h is None or h["stage"].numel() < sum(sizes) or h["dev"].numel() != n_t:
+            h = self._frames = {
+                "dev": torch.empty(n_t, dtype=torch.float32, device="cuda"),
+                "stage": torch.empty(max(sum(sizes), 1), dtype=torch.uint8, device="cuda"),
+                "stream": torch.cuda.Stream(),
+                "ready": torch.cuda.Event(),
+                "free": torch.cuda.Event(),
+            }
+            self._frames_prefetched = None
+
+        def upload(src):
+            for f, o, nb in zip(src, offs, sizes):
+                h["stage"][o:o + nb].copy_(f.reshape(-1), non_blocking=True)
+
+        pre = self._frames_prefetched
+        if pre is not None and len(pre) == len(frames) and all(a is b for a, b in zip(pre, frames)):
+            main.wait_event(h["ready"])
+        else:
+            upload(frames)
+        self.ctx.frames_to_targets(h["stage"], descs, cams, out=h["dev"])
+        h["free"].record(main)  # the staging bytes have been read
+        loss = self.train_step(cams, h["dev"], iteration)
+        self._frames_prefetched = None
+        if next_frames is not None:
+            nxt = list(next_frames)
+            if [tuple(f.shape) for f in nxt] != [tuple(f.shape) for f in frames]:
+                raise ValueError("next frames must have the shapes of this step's frames")
+            for f in nxt:
+                if f.dtype != torch.uint8 or not f.is_pinned():
+                    raise ValueError("frames must be pinned [H,W,3] uint8 tensors")
+            cs = h["stream"]
+            cs.wait_event(h["free"])
+            with torch.cuda.stream(cs):
+                upload(nxt)
+            h["ready"].record(cs)
+            self._frames_prefetched = nxt  # held, so the identity check above stays sound
+        return loss
 
     def train_step_host(self, cameras, host_targets: torch.Tensor, iteration: int, next_host_targets=None):
         """One step whose targets live in pinned host memory.

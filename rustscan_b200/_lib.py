@@ -122,6 +122,10 @@ class gsr_topo_params(C.Structure):
                 ("train_t", C.c_float), ("opacity_reset", C.c_int32), ("opacity_reset_cap", C.c_float)]
 
 
+class gsr_frame(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
 GSR_TUNE_CANDIDATES = 9
 
 
@@ -149,6 +153,7 @@ EXPORTED = [
     "gsr_render_backward",
     "gsr_export",
     "gsr_loss",
+    "gsr_frames_to_targets",
     "gsr_adam_step",
     "gsr_accumulate_densify",
     "gsr_train_step",
@@ -196,6 +201,7 @@ def load():
     L.gsr_render_backward.argtypes = [vp, C.POINTER(gsr_splats), vp, C.POINTER(gsr_grads), vp, vp]
     L.gsr_export.argtypes = [vp, u32, i32, vp, C.c_uint64, vp]
     L.gsr_loss.argtypes = [vp, vp, vp, C.POINTER(gsr_camera), u32, f32, f32, vp, vp, vp]
+    L.gsr_frames_to_targets.argtypes = [vp, vp, C.POINTER(gsr_frame), C.POINTER(gsr_camera), u32, vp, vp]
     L.gsr_adam_step.argtypes = [vp, vp, vp, vp, u32, u32, C.POINTER(gsr_grads), C.POINTER(gsr_adam_state),
                                 C.POINTER(gsr_lr), i32, vp]
     L.gsr_accumulate_densify.argtypes = [vp, C.POINTER(gsr_grads), vp, vp, u32, u32, i32, vp, vp]

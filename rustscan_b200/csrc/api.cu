@@ -550,6 +550,26 @@ gsr_status gsr_export(gsr_ctx* c, uint32_t view, int32_t what, void* dst, uint64
   return GSR_OK;
 }
 
+gsr_status gsr_frames_to_targets(gsr_ctx* c, const uint8_t* frames, const gsr_frame* desc, const gsr_camera* cams,
+                                 uint32_t n_views, float* targets, void* stream) {
+  if (!c) return GSR_ERR_INVALID_ARG;
+  if (n_views == 0) return GSR_OK;
+  if (!frames || !desc || !cams || !targets) return fail(c, GSR_ERR_INVALID_ARG, "null frame or target buffer");
+  if (n_views > (uint32_t)kMaxViews) return fail(c, GSR_ERR_INVALID_ARG, "at most 64 frames per call");
+  std::vector<FrameSpec> spec(n_views);
+  for (uint32_t v = 0; v < n_views; ++v) {
+    if (desc[v].width == 0 || desc[v].height == 0) return fail(c, GSR_ERR_INVALID_ARG, "empty frame");
+    if (cams[v].width == 0 || cams[v].height == 0) return fail(c, GSR_ERR_INVALID_ARG, "empty target view");
+    spec[v].src_offset = desc[v].offset;
+    spec[v].src_w = desc[v].width;
+    spec[v].src_h = desc[v].height;
+    spec[v].dst_w = cams[v].width;
+    spec[v].dst_h = cams[v].height;
+  }
+  GSR_CUDA(c, launch_frames_to_targets(frames, spec.data(), n_views, targets, (cudaStream_t)stream));
+  return GSR_OK;
+}
+
 gsr_status gsr_loss(gsr_ctx* c, const float* pred, const float* target, const gsr_camera* cams, uint32_t n_views,
                     float l1_w, float ssim_w, float* loss, float* v_pred, void* stream) {
   if (!c) return GSR_ERR_INVALID_ARG;

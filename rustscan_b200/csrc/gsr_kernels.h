@@ -166,6 +166,15 @@ cudaError_t launch_set_views(ViewDesc* dst, const ViewDesc* host, uint32_t n, cu
 
 cudaError_t launch_visible_out(const ViewSet& vs, FwdBufs& b, uint32_t n, float* out_visible, cudaStream_t st);
 
+// 8-bit RGB frames to f32 training targets (views packed back to back).
+struct FrameSpec {
+  uint64_t src_offset;     // byte offset of the frame in the frame buffer
+  uint32_t src_w, src_h;   // frame size
+  uint32_t dst_w, dst_h;   // training resolution of the view
+};
+cudaError_t launch_frames_to_targets(const uint8_t* frames, const FrameSpec* spec, uint32_t n_views, float* out,
+                                     cudaStream_t st);
+
 // Per-step optimizer scalars, read by the kernels from device memory so that
 // a captured step can be replayed with new values.
 struct AdamScalars {

@@ -53,6 +53,7 @@ def test_struct_layouts_match_header():
         "gsr_tune_result": _lib.gsr_tune_result,
         "gsr_topo_row": _lib.gsr_topo_row,
         "gsr_topo_params": _lib.gsr_topo_params,
+        "gsr_frame": _lib.gsr_frame,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
