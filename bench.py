@@ -328,7 +328,11 @@ def main():
     gts = host_splats_to_device(S.Scene(gt_tr, gt_sh, gt_op, 3, cams))
     fit_capacity(ctx, gts, cams)
     flat, _, _ = ctx.render_forward(gts, cams)
-    targets = flat.view(nv, H, W, 4)[..., :3].contiguous()
+    # The training frames are 8-bit RGB images (what a camera or the dataset
+    # decoder gives); the device targets are their conversion on the GPU.
+    frames_u8 = (flat.view(nv, H, W, 4)[..., :3].clamp(0, 1) * 255.0).round().to(torch.uint8).contiguous()
+    targets = ctx.frames_to_targets(frames_u8.view(-1), [(v * H * W * 3, W, H) for v in range(nv)],
+                                    cams).view(nv, H, W, 3)
     del gts
     fit_capacity(ctx, splats, cams)
     counts = [ctx.export(v, "counts") for v in range(nv)]
@@ -400,23 +404,26 @@ def main():
         ctx1.close()
 
     # ---- end to end through the public API with host buffers -------------------
-    host_t = torch.empty(targets.shape, dtype=torch.float32, pin_memory=True)
-    host_t.copy_(targets.cpu())
+    # The step's inputs are the views' 8-bit frames in pinned host memory;
+    # Trainer.train_step_frames uploads them and converts them on the device.
+    host_frames = [torch.empty((H, W, 3), dtype=torch.uint8, pin_memory=True) for _ in range(nv)]
+    for v in range(nv):
+        host_frames[v].copy_(frames_u8[v].cpu())
     host_loss = torch.empty(nv, dtype=torch.float32, pin_memory=True)
     e2e_warm = 1
 
     def e2e_step(it):
-        # Each timed step's targets cross PCIe once: the first timed step
+        # Each timed step's frames cross PCIe once: the first timed step
         # copies its own, every other one was prefetched by the step before
         # it (inside the timed region); the warm-up and the last timed step
         # prefetch nothing.
-        nxt = host_t if e2e_warm < it < e2e_warm + args.steps else None
-        loss = trainer.train_step_host(cams, host_t, it, next_host_targets=nxt)
+        nxt = host_frames if e2e_warm < it < e2e_warm + args.steps else None
+        loss = trainer.train_step_frames(cams, host_frames, it, next_frames=nxt)
         host_loss.copy_(loss, non_blocking=True)
 
     ms_e2e = time_steps(e2e_step, args.steps, e2e_warm, world) / args.steps
-    e2e = {"value": ms_e2e / nv, "unit": UNIT, "h2d_bytes_per_step": int(host_t.numel() * 4),
-           "d2h_bytes_per_step": int(nv * 4)}
+    e2e = {"value": ms_e2e / nv, "unit": UNIT, "h2d_bytes_per_step": int(sum(f.numel() for f in host_frames)),
+           "d2h_bytes_per_step": int(nv * 4), "inputs": "8-bit RGB frames, converted to f32 targets on the device"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
