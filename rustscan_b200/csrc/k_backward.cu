@@ -39,7 +39,7 @@ struct NoCoeff {
   __device__ float operator()(int, int) const { return 0.f; }
 };
 
-__global__ void __launch_bounds__(128) pair_bwd_kernel(PairArgs a) {
+__global__ void __launch_bounds__(128, 6) pair_bwd_kernel(PairArgs a) {
   const uint32_t v = blockIdx.y;
   const uint32_t V = a.b.vcount[v * 4 + 0];
   const ViewDesc& vd = a.vs.views[v];
