@@ -88,7 +88,7 @@ struct SortPassArgs {
 
 // KV: values travel with the keys; otherwise the keys are sorted alone.
 template <bool KV>
-__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassArgs a) {
+__global__ void __launch_bounds__(kSortThreads, KV ? 2 : 3) sort_pass_kernel(SortPassArgs a) {
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[KV ? kSortTile : 1];
   __shared__ uint32_t s_whist[kSortWarps][256];
