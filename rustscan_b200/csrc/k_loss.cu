@@ -52,7 +52,7 @@ struct SsimFwdSmem {
   float red[2][8];
 };
 
-__global__ void __launch_bounds__(kLT) ssim_fwd_kernel(LossArgs a) {
+__global__ void __launch_bounds__(kLT, 5) ssim_fwd_kernel(LossArgs a) {
   extern __shared__ float4 smem_raw[];
   SsimFwdSmem& S = *reinterpret_cast<SsimFwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
@@ -214,7 +214,7 @@ struct SsimBwdSmem {
   float v[3][LTY][HX];
 };
 
-__global__ void __launch_bounds__(kLT) ssim_bwd_kernel(LossArgs a) {
+__global__ void __launch_bounds__(kLT, 5) ssim_bwd_kernel(LossArgs a) {
   extern __shared__ float4 smem_raw[];
   SsimBwdSmem& S = *reinterpret_cast<SsimBwdSmem*>(smem_raw);
   const uint32_t v = blockIdx.z, ch = blockIdx.y;
