@@ -96,12 +96,14 @@ __device__ __forceinline__ uint32_t stage_one(const float4* rec, uint32_t c, flo
   return mask;
 }
 
-// Order-preserving compaction of the batch entries whose mask has bit w.
-__device__ __forceinline__ int build_list(const uint8_t* s_mask, uint32_t nb, int w, int lane, uint16_t* list) {
+// Order-preserving compaction of the batch entries whose mask has a bit of
+// wsel.
+__device__ __forceinline__ int build_list(const uint8_t* s_mask, uint32_t nb, uint32_t wsel, int lane,
+                                          uint16_t* list) {
   int cnt = 0;
   for (uint32_t base = 0; base < nb; base += 32) {
     const uint32_t j = base + lane;
-    const bool bit = j < nb && ((s_mask[j] >> w) & 1u);
+    const bool bit = j < nb && (s_mask[j] & wsel) != 0u;
     const uint32_t bal = __ballot_sync(0xffffffffu, bit);
     if (bit) list[cnt + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)j;
     cnt += __popc(bal);
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     }
     __syncthreads();
     if (!__all_sync(0xffffffffu, all_done)) {
-      const int cnt = build_list(s_mask, nb, warp, lane, s_list[warp]);
+      const int cnt = build_list(s_mask, nb, 1u << warp, lane, s_list[warp]);
       // Entries go two at a time: the sigma, cut test, exponential and
       // contribution test of both (independent of the pixel state) form one
       // straight-line block whose chains interleave; the blends then apply
@@ -516,6 +518,14 @@ __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, floa
 // per lane) onto the warp blocks of a backward with PB pixels per lane: a
 // backward block is the union of the forward blocks of its column span and
 // rows.
+// The forward warp block (8x8 pixels) that holds pixel pair k of backward
+// warp w with PB pixels per lane (its rows 8k .. 8k + 7).
+template <int TW, int PB>
+__device__ __forceinline__ int fwd_block_of(int w, int k) {
+  constexpr int KX = TW / 8;
+  return (w % KX) + ((w / KX) * (PB / 2) + k) * KX;
+}
+
 template <int TW, int TH, int PB>
 __device__ __forceinline__ uint32_t hit_bits_for(uint32_t f) {
   constexpr int PF = kFwdPPL;
@@ -585,6 +595,9 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   if (lane == 0) atomicMax(&s_max, wmax);
   __syncthreads();
   const uint32_t smax = s_max;
+  uint32_t wsel = 0;  // the forward blocks inside this warp's block
+#pragma unroll
+  for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
   auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
   // List entries [lo, hi) of a batch into registers.
   uint32_t pc[kSI], ph[kSI];
@@ -604,9 +617,8 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     for (int it = 0; it < kSI; ++it) {
       const uint32_t j = threadIdx.x + it * NT;
       if (j < (uint32_t)BATCH && lo + j < hi) {
-        const uint32_t hm = hit_bits_for<TW, TH, PPL>(ph[it]);
-        s_mask[buf][j] = (uint8_t)hm;
-        if (hm) {
+        s_mask[buf][j] = (uint8_t)ph[it];  // the forward's 8x8 block bits
+        if (ph[it]) {
           s_cidx[buf][j] = pc[it];
           const float4* r = rec + (size_t)pc[it] * 3;
           cp_async16(&s_rec[buf][j][0], r);
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     cp_async_wait1();  // this thread's copies of the current batch have landed
     __syncthreads();
     if (bs < wmax) {
-      const int cnt = build_list(s_mask[buf], nb, warp, lane, s_list[warp]);
+      const int cnt = build_list(s_mask[buf], nb, wsel, lane, s_list[warp]);
       for (int e = cnt - 1; e >= 0; --e) {
         const uint32_t j = s_list[warp][e];
         const uint32_t s = bs + j;
@@ -654,20 +666,21 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
         acc.ax = acc.ay = 0.f;
         acc.n = 0u;
         const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
-        PairPre pre[NP];
-        uint32_t need = 0;  // pairs with a pixel that can take the Gaussian, over the warp
+        // The pairs of this warp whose 8x8 block had a pixel take the
+        // Gaussian in the forward (the others contribute nothing here).
+        const uint32_t mraw = s_mask[buf][j];
+        uint32_t need = 0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-          const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
-          pre[k] = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
-          if (__any_sync(0xffffffffu, pre[k].l0 || pre[k].l1)) need |= 1u << k;
-        }
-        // Pairs needed by the warp run as one straight-line block, so that
-        // their independent instruction chains interleave.
+        for (int k = 0; k < NP; ++k)
+          if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) need |= 1u << k;
+        // The needed pairs run as one straight-line block (need is
+        // warp-uniform), so that their independent chains interleave.
         auto rest = [&](int k) {
+          const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
+          const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
           const float2 cpv =
               fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
-          bwd_pair_rest<REF>(pp[k], pre[k], adx, bdx, cb, B, cpv, acc);
+          bwd_pair_rest<REF>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
         };
         if constexpr (NP == 2) {
           if (need == 3u) {
@@ -710,7 +723,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < nb * 3; q += NT) {
       const uint32_t j = q / 3, k = q % 3;
-      const uint32_t m = s_mask[buf][j];
+      const uint32_t m = hit_bits_for<TW, TH, PPL>(s_mask[buf][j]);  // warps that wrote a slot
       float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
       bool any = false;
 #pragma unroll
