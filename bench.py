@@ -376,8 +376,8 @@ def main():
     # intersections), scaled to the launch by its intersections (the raster
     # and tile-sort traffic grows with them) or, for Adam, taken as is (it
     # sweeps the N parameters once per step).
-    traffic_coeff = {"raster_bwd": (37.742e6 + 0.023e6) / 6273269, "raster_fwd": (14.117e6 + 0.142e6) / 6273269,
-                     "tile_sort": (27.618e6 + 0.427e6 + 27.366e6 + 0.415e6) / 6273269}
+    traffic_coeff = {"raster_bwd": (37.752e6 + 0.012e6) / 6273269, "raster_fwd": (14.120e6 + 0.117e6) / 6273269,
+                     "tile_sort": (27.630e6 + 0.043e6 + 27.734e6 + 0.063e6) / 6273269}
     if dom in traffic_coeff:
         traffic = traffic_coeff[dom] * sum(I)
     elif dom == "adam":
