@@ -29,6 +29,7 @@ struct WalkWarp {
   uint32_t run[32];  // passing tiles found so far, per Gaussian
   uint32_t off[32];  // emission offset, per Gaussian
   uint32_t cid[32];  // compact index, per Gaussian
+  uint32_t lane_of_rank[32];  // lanes of the Gaussians with a non-empty box, in lane order
 };
 
 constexpr int kWalkThreads = 256;
@@ -109,24 +110,25 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
     S.run[lane] = 0u;
     S.off[lane] = o0;
     S.cid[lane] = c;
+    const uint32_t nzm = __ballot_sync(0xffffffffu, nb > 0u);
+    if (nb > 0u) S.lane_of_rank[__popc(nzm & ((1u << lane) - 1u))] = lane;
     __syncwarp();
+    const uint32_t ex = incl - nb;
     for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
       const uint32_t t = t0 + lane;
       const bool live = t < total;
+      // Owner of item t: the Gaussians with a non-empty box own consecutive
+      // item runs. The run starts inside [t0, t0 + 32) mark bits; the owner of
+      // t0 is the first Gaussian whose run ends after t0, and every start at
+      // positions 1..lane moves the owner of t0 + lane one Gaussian further.
+      const uint32_t sbit = (nb > 0u && ex >= t0 && ex < t0 + 32u) ? (1u << (ex - t0)) : 0u;
+      const uint32_t starts = __reduce_or_sync(0xffffffffu, sbit);
+      const uint32_t r0 = (uint32_t)__popc(__ballot_sync(0xffffffffu, nb > 0u && incl <= t0));
       uint32_t owner = 0u, tx = 0u, ty = 0u;
       bool pass = false;
       if (live) {
-        // The first Gaussian whose inclusive prefix exceeds t (exists: t < total).
-        uint32_t lo = 0u, hi = 31u;
-#pragma unroll
-        for (int s = 0; s < 5; ++s) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (S.incl[mid] > t)
-            hi = mid;
-          else
-            lo = mid + 1u;
-        }
-        owner = lo;
+        const uint32_t upto = ((2u << lane) - 1u) & ~1u;  // positions 1..lane
+        owner = S.lane_of_rank[r0 + (uint32_t)__popc(starts & upto)];
         const uint32_t local = t - S.ex[owner];
         const uint32_t ow = S.w[owner];
         const uint32_t ry = local / ow;
