@@ -24,7 +24,7 @@
 // contributor by division (T_i = T_{i+1} / (1 - alpha_i)), keeps the colour
 // accumulated behind it, and forms per-pixel gradients (blend_step_grad).
 // Per Gaussian the gradient sums over a warp's pixels come from a
-// reduce-scatter butterfly (16 shuffles), over the CTA's warps from shared
+// reduce-scatter butterfly (13 shuffles), over the CTA's warps from shared
 // memory in warp order, and over tiles from float4 atomics (or, in
 // deterministic mode, per-intersection records reduced later in a fixed
 // order).
@@ -349,38 +349,52 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   }
 }
 
-// Reduce-scatter of 16 per-lane values over the warp: returns in every lane
-// the warp total of slot (lane >> 1). Summation order is fixed.
-__device__ __forceinline__ float warp_reduce_scatter16(float (&x)[16], int lane) {
+// Reduce-scatter of 12 per-lane values over the warp in 13 shuffles. Lane
+// l ends with the warp total of value reduce12_slot(l) (lanes whose bit 1 is
+// set and bit 2 differs hold the same value; the fixed summation order makes
+// them equal). Stages: xor 16 halves 12 -> 6, xor 8 halves 6 -> 3, xor 4
+// splits values 0 and 2 and sums value 1 in both lanes, xor 2 splits the two
+// left, xor 1 completes the sum.
+__device__ __forceinline__ int reduce12_slot(int lane) {
+  const int g16 = (lane >> 4) & 1, g8 = (lane >> 3) & 1, g4 = (lane >> 2) & 1, g2 = (lane >> 1) & 1;
+  return (g2 ? 1 : (g4 ? 2 : 0)) + 3 * g8 + 6 * g16;
+}
+__device__ __forceinline__ float warp_reduce_scatter12(float (&x)[12], int lane) {
   const uint32_t full = 0xffffffffu;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  {
     const bool hi = lane & 16;
-    const float send = hi ? x[i] : x[i + 8];
-    const float keep = hi ? x[i + 8] : x[i];
-    x[i] = keep + __shfl_xor_sync(full, send, 16);
-  }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const bool hi = lane & 8;
-    const float send = hi ? x[i] : x[i + 4];
-    const float keep = hi ? x[i + 4] : x[i];
-    x[i] = keep + __shfl_xor_sync(full, send, 8);
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const bool hi = lane & 4;
-    const float send = hi ? x[i] : x[i + 2];
-    const float keep = hi ? x[i + 2] : x[i];
-    x[i] = keep + __shfl_xor_sync(full, send, 4);
+    for (int i = 0; i < 6; ++i) {
+      const float send = hi ? x[i] : x[i + 6];
+      const float keep = hi ? x[i + 6] : x[i];
+      x[i] = keep + __shfl_xor_sync(full, send, 16);
+    }
   }
   {
-    const bool hi = lane & 2;
-    const float send = hi ? x[0] : x[1];
-    const float keep = hi ? x[1] : x[0];
-    x[0] = keep + __shfl_xor_sync(full, send, 2);
+    const bool hi = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float send = hi ? x[i] : x[i + 3];
+      const float keep = hi ? x[i + 3] : x[i];
+      x[i] = keep + __shfl_xor_sync(full, send, 8);
+    }
   }
-  return x[0] + __shfl_xor_sync(full, x[0], 1);
+  float w0, w1;
+  {
+    const bool hi = lane & 4;
+    const float send = hi ? x[0] : x[2];
+    const float keep = hi ? x[2] : x[0];
+    w0 = keep + __shfl_xor_sync(full, send, 4);
+    w1 = x[1] + __shfl_xor_sync(full, x[1], 4);
+  }
+  float u;
+  {
+    const bool hi = lane & 2;
+    const float send = hi ? w0 : w1;
+    const float keep = hi ? w1 : w0;
+    u = keep + __shfl_xor_sync(full, send, 2);
+  }
+  return u + __shfl_xor_sync(full, u, 1);
 }
 
 // Per-pair state of the reverse walk (pixel q = 2k + h is half h of pair k).
@@ -595,6 +609,8 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   if (lane == 0) atomicMax(&s_max, wmax);
   __syncthreads();
   const uint32_t smax = s_max;
+  const int slot = reduce12_slot(lane);                          // the gradient value this lane ends with
+  const bool writer = (lane & 1) == 0 && !((lane & 2) && (lane & 4));  // one lane per value
   uint32_t wsel = 0;  // the forward blocks inside this warp's block
 #pragma unroll
   for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
@@ -697,7 +713,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
             if (need & (1u << k)) rest(k);
         }
         const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
-        float x[16];
+        float x[12];
         x[0] = adx * M0 + cb * M1;
         x[1] = bdx * M0 + B.x * M1;
         x[2] = (0.5f * dx * dx) * M0;
@@ -710,14 +726,11 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
         x[9] = acc.ax;
         x[10] = acc.ay;
         x[11] = (float)acc.n;
-#pragma unroll
-        for (int i = 12; i < 16; ++i) x[i] = 0.f;
-        float r = warp_reduce_scatter16(x, lane);
-        const int slot = lane >> 1;
+        float r = warp_reduce_scatter12(x, lane);
         // v_rgb is zero for a channel whose raw colour is negative.
         if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
         float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
-        if ((lane & 1) == 0 && slot < 12) sp[slot] = r;
+        if (writer) sp[slot] = r;
       }
     }
     __syncthreads();
