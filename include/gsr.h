@@ -109,8 +109,12 @@ GSR_API const char* gsr_version(void);
 
 /* Synchronises the stream, then reports device-side conditions of the work
  * enqueued so far: GSR_ERR_CAPACITY with *required set to the intersection
- * count that did not fit, GSR_ERR_TIMEOUT if a bounded wait gave up.
- * Clears the conditions. Host-synchronising. */
+ * capacity that did not fit, GSR_ERR_TIMEOUT if a bounded wait gave up.
+ * Clears the conditions. Host-synchronising. The capacity counts the
+ * binning's slots: the intersections themselves, or, when the tile id and
+ * the compact index pack into one 32-bit key with a tile id to spare (the
+ * common case, no counting pass), every tile of each visible Gaussian's
+ * tile box. */
 GSR_API gsr_status gsr_sync_status(gsr_ctx* ctx, void* stream, uint64_t* required);
 
 /* Grows the per-view intersection capacity (frees and reallocates scratch;

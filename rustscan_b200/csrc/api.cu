@@ -290,10 +290,6 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   prof_mark(c, kStDepthSort, st);
   GSR_CUDA(c, radix_sort_pairs(b.depth_key, nullptr, b.depth_sorted, b.perm, b.key_tmp, b.val_tmp, b.Vcap, n_views,
                                b.vcount, 4, 0, b.Vcap, 31, c->s, st));
-  prof_mark(c, kStOffsets, st);
-  GSR_CUDA(c, launch_count(vs, b, c->s, st));
-  GSR_CUDA(c, launch_offsets(vs, b, c->s, st));
-  prof_mark(c, kStEmit, st);
   // Up to kHistMaxTiles tiles a view, emission also counts intersections
   // per tile: the tile ranges and the tile sort's digit histograms follow
   // from those counts (no histogram pass, no ranges pass).
@@ -303,16 +299,24 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   // one packed key (tile id high, index low), sorted alone.
   const int tbits = bits_for(vs.max_tiles), ibits = bits_for(sp->n);
   b.pack_bits = (tile_counts && !c->cfg.deterministic && tbits + ibits <= 32) ? (uint32_t)ibits : 0u;
+  // Packed keys with a spare tile id use the slot layout: every box tile
+  // gets a slot (offsets from the box sizes the projection wrote), failing
+  // tiles hold a sentinel key that sorts last, and no counting walk runs.
+  b.slots = b.pack_bits != 0 && vs.max_tiles < (1u << tbits);
+  prof_mark(c, kStOffsets, st);
+  if (!b.slots) GSR_CUDA(c, launch_count(vs, b, c->s, st));
+  GSR_CUDA(c, launch_offsets(vs, b, c->s, st));
+  prof_mark(c, kStEmit, st);
   if (tile_counts) {
-    GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, st));
-    GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, tbits, st));
+    GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, b.slots, st));
+    GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, tbits, b.slots, st));
   } else {
     GSR_CUDA(c, launch_emit(vs, b, c->s, c->cfg.deterministic, st));
   }
   prof_mark(c, kStTileSort, st);
   if (b.pack_bits)
     GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, nullptr, b.isect_key, nullptr, b.key_tmp, nullptr, b.Icap, n_views,
-                                 b.vcount + 1, 4, 0, b.Icap, tbits, c->s, st, true, b.pack_bits));
+                                 b.vcount + (b.slots ? 3 : 1), 4, 0, b.Icap, tbits, c->s, st, true, b.pack_bits));
   else
     GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, b.isect_val_raw, b.isect_key, b.isect_val, b.key_tmp, b.val_tmp,
                                  b.Icap, n_views, b.vcount + 1, 4, 0, b.Icap, tbits, c->s, st, tile_counts));
@@ -540,7 +544,13 @@ gsr_status gsr_export(gsr_ctx* c, uint32_t view, int32_t what, void* dst, uint64
     case 8: src = slice(b.ncontrib, b.Pcap, view); need = 4 * P; break;
     case 9: src = slice(b.sgrad, b.Vcap * 3, view); need = 48 * V; break;
     case 10: src = slice(b.nvisit, b.Pcap, view); need = 4 * P; break;
-    case 11: src = slice(b.count, b.Vcap, view); need = 4 * V; break;
+    case 11:
+      // The slot layout keeps box sizes there; the passing-tile counts are
+      // recounted from the sorted intersections.
+      if (b.slots) GSR_CUDA(c, launch_count_from_isects(b, view, (uint32_t)V, st));
+      src = slice(b.count, b.Vcap, view);
+      need = 4 * V;
+      break;
     case 12: src = slice(b.hitw, b.Icap, view); need = I; break;
     default: return fail(c, GSR_ERR_INVALID_ARG, "unknown export selector");
   }

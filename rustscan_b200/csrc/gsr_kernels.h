@@ -46,6 +46,7 @@ struct FwdBufs {
   uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
   uint64_t Vcap, Ncap, Icap, Tcap, Pcap;
   uint32_t pack_bits;      // > 0: intersections are packed keys (see isect_key), else (tile, index) pairs
+  bool slots;              // slot layout: one key per box tile, sentinel keys last; vcount[3] = keys sorted
 };
 
 // The compact index of intersection s (packed keys or pairs).
@@ -140,10 +141,17 @@ cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int det
 // histograms (Scratch::hist), replacing the sort's histogram pass and the
 // ranges kernel. For views of at most kHistMaxTiles tiles.
 constexpr uint32_t kHistMaxTiles = 8192;
-cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st);
+// slots: the slot layout (offsets from box sizes, failing tiles write the
+// sentinel key); packed keys only.
+cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, bool slots,
+                             cudaStream_t st);
 // Tile ranges and the tile sort's digit histograms (digits of
 // sort_digit_bits(bits_for(max tiles)) bits) from emission's tile counts.
-cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, cudaStream_t st);
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, bool slots,
+                                   cudaStream_t st);
+// Packed mode only: the passing-tile counts of a view's compact indices,
+// recounted from its sorted intersections into b.count.
+cudaError_t launch_count_from_isects(FwdBufs& b, uint32_t view, uint32_t n_visible, cudaStream_t st);
 // Packed mode only: intersections [0, n) of a view as separate tile ids and
 // compact indices.
 cudaError_t launch_unpack_isects(const FwdBufs& b, uint32_t view, uint32_t n, uint32_t* tiles, uint32_t* vals,

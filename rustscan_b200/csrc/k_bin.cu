@@ -41,7 +41,11 @@ constexpr int kWalkWarps = kWalkThreads / 32;
 // Gaussian's scanned offset; then replace the record's tile box with the
 // footprint half-widths the rasterizer culls warp blocks with (negative: no
 // box, never cull).
-template <bool EMIT, bool HIST = false>
+// SLOTS (emission only): every box tile of a Gaussian has a slot at its
+// row-major position after the Gaussian's offset (offsets scanned from box
+// sizes, no counting walk); a passing tile writes its packed key there, a
+// failing one the all-ones key, which sorts after every tile.
+template <bool EMIT, bool HIST = false, bool SLOTS = false>
 __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, FwdBufs b, int det) {
   __shared__ WalkWarp s_w[kWalkWarps];
   extern __shared__ uint32_t s_th[];  // HIST: per-tile counts of this block's emitted intersections
@@ -124,18 +128,32 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
       const uint32_t sbit = (nb > 0u && ex >= t0 && ex < t0 + 32u) ? (1u << (ex - t0)) : 0u;
       const uint32_t starts = __reduce_or_sync(0xffffffffu, sbit);
       const uint32_t r0 = (uint32_t)__popc(__ballot_sync(0xffffffffu, nb > 0u && incl <= t0));
-      uint32_t owner = 0u, tx = 0u, ty = 0u;
+      uint32_t owner = 0u, tx = 0u, ty = 0u, local = 0u;
       bool pass = false;
       if (live) {
         const uint32_t upto = ((2u << lane) - 1u) & ~1u;  // positions 1..lane
         owner = S.lane_of_rank[r0 + (uint32_t)__popc(starts & upto)];
-        const uint32_t local = t - S.ex[owner];
+        local = t - S.ex[owner];
         const uint32_t ow = S.w[owner];
         const uint32_t ry = local / ow;
         tx = S.x0[owner] + (local - ry * ow);
         ty = S.y0[owner] + ry;
         pass = will_primitive_contribute(tx, ty, ts, V2<float>{S.mx[owner], S.my[owner]},
                                          V3<float>{S.ca[owner], S.cb[owner], S.cc[owner]}, S.thr[owner]);
+      }
+      if (SLOTS) {
+        if (live) {
+          const uint64_t o = (uint64_t)S.off[owner] + local;
+          if (o < cap) {
+            if (pass) {
+              if (HIST) atomicAdd(&s_th[tx + ty * vd.tiles_x], 1u);
+              keys[o] = ((tx + ty * vd.tiles_x) << b.pack_bits) | S.cid[owner];
+            } else {
+              keys[o] = 0xffffffffu;
+            }
+          }
+        }
+        continue;
       }
       const uint32_t pm = __ballot_sync(0xffffffffu, pass);
       const uint32_t prev = __shfl_up_sync(0xffffffffu, owner, 1);
@@ -193,7 +211,8 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
 // tile id's digits, in the sort's histogram layout.
 constexpr int kHistThreads = 1024;
 __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist,
-                                                                         uint32_t dbits) {
+                                                                         uint32_t dbits, uint32_t sentinel_tile,
+                                                                         int slots) {
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_h[2][256];
   const uint32_t v = blockIdx.x;
@@ -227,6 +246,18 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
     }
     run += loc[i];
   }
+  if (slots && threadIdx.x == 0) {
+    // Slot layout: the sort covers every slot written (the scanned box
+    // sizes, clamped to capacity); the slots of failing tiles hold the
+    // sentinel tile. The view's intersection count becomes the real one.
+    const uint32_t written = b.vcount[v * 4 + 1];
+    const uint32_t dm = (1u << dbits) - 1u;
+    atomicAdd(&s_h[0][sentinel_tile & dm], written - all);
+    atomicAdd(&s_h[1][(sentinel_tile >> dbits) & dm], written - all);
+    b.vcount[v * 4 + 3] = written;
+    b.vcount[v * 4 + 1] = all;
+    b.vcount[v * 4 + 2] = all;
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < 1024; i += kHistThreads) {
     const int p = i >> 8;
@@ -258,6 +289,15 @@ __global__ void __launch_bounds__(256) unpack_isects_kernel(const uint32_t* pack
     tiles[s] = k >> bits;
     vals[s] = k & ((1u << bits) - 1u);
   }
+}
+
+// Passing-tile counts per compact index from the sorted packed keys of one
+// view (the slot layout has no counting walk); count must be zeroed.
+__global__ void __launch_bounds__(256) count_from_isects_kernel(const uint32_t* keys, const uint32_t* n_isects,
+                                                                uint32_t mask, uint32_t* count) {
+  const uint32_t n = *n_isects;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+    atomicAdd(count + (keys[s] & mask), 1u);
 }
 
 // get_tile_offsets.wgsl:11-30. ranges must be zeroed beforehand.
@@ -346,18 +386,35 @@ cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int det
   return cudaGetLastError();
 }
 
-cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, cudaStream_t st) {
+cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, bool slots,
+                             cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
+  if (slots && (deterministic || !b.pack_bits)) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(b.tile_hist, 0, sizeof(uint32_t) * b.Tcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   const size_t smem = sizeof(uint32_t) * vs.max_tiles;
-  tile_walk_kernel<true, true><<<grid_for(vs, s.num_sms), kWalkThreads, smem, st>>>(vs, b, deterministic);
+  if (slots)
+    tile_walk_kernel<true, true, true><<<grid_for(vs, s.num_sms), kWalkThreads, smem, st>>>(vs, b, 0);
+  else
+    tile_walk_kernel<true, true><<<grid_for(vs, s.num_sms), kWalkThreads, smem, st>>>(vs, b, deterministic);
   return cudaGetLastError();
 }
 
-cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, cudaStream_t st) {
+cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, bool slots,
+                                   cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles || sort_passes(tile_bits) > 2) return cudaErrorInvalidValue;
-  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits));
+  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits),
+                                                                (1u << tile_bits) - 1u, slots ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_from_isects(FwdBufs& b, uint32_t view, uint32_t n_visible, cudaStream_t st) {
+  if (!b.pack_bits) return cudaErrorInvalidValue;
+  uint32_t* count = slice(b.count, b.Vcap, view);
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * n_visible, st);
+  if (e != cudaSuccess) return e;
+  count_from_isects_kernel<<<1024, 256, 0, st>>>(slice(b.isect_key, b.Icap, view), b.vcount + view * 4 + 1,
+                                                 (1u << b.pack_bits) - 1u, count);
   return cudaGetLastError();
 }
 

@@ -224,6 +224,10 @@ __global__ void __launch_bounds__(kProjThreads) records_kernel(ProjectArgs a) {
                          __uint_as_float(p.box.y0 | (p.box.y1 << 16)));
       slice(a.b.gid_of_c, a.b.Vcap, v)[c] = g;
       slice(a.b.depth_key, a.b.Vcap, v)[c] = __float_as_uint(p.depth);
+      // Tiles of the box: the intersection slots of the slot layout (the
+      // counting walk replaces them by passing-tile counts otherwise).
+      const uint32_t bw = p.box.x1 > p.box.x0 ? p.box.x1 - p.box.x0 : 0u;
+      slice(a.b.count, a.b.Vcap, v)[c] = bw * (p.box.y1 > p.box.y0 ? p.box.y1 - p.box.y0 : 0u);
     }
   }
 }

@@ -111,7 +111,13 @@ def test_capacity_overflow_reported_then_fixed(gsr_ctx_factory):
     with pytest.raises(GsrError) as ei:
         ctx.render_forward(splats, sc.cameras, check=True)
     o = oracle_forward(sc, sc.cameras[0])
-    assert ei.value.status == 3 and ei.value.required == o.num_intersections
+    # The required capacity counts the binning's intersection slots: with
+    # packed keys and a spare tile id, one per tile of each visible
+    # Gaussian's tile box (the passing tiles among them are the intersections).
+    b = o.box.astype(np.int64)
+    slots = int((np.maximum(b[:, 2] - b[:, 0], 0) * np.maximum(b[:, 3] - b[:, 1], 0)).sum())
+    assert slots >= o.num_intersections
+    assert ei.value.status == 3 and ei.value.required == slots
     ctx.reserve_isects(ei.value.required)
     _, g = run_gpu_forward(ctx, splats, sc.cameras)
     torch.cuda.synchronize()
