@@ -68,11 +68,11 @@ template <int TW, int PPL> struct WarpBlock {
   __device__ static int y0(int w) { return (w / kWarpsX) * kRows; }
 };
 
-// Stages one Gaussian: records in shared memory plus the bit mask of warp
-// blocks its padded footprint box overlaps (half-widths written by the
-// emission kernel into r2.zw; negative means no box, never cull). The
-// forward stages colours clamped at zero, the backward raw colours.
-template <int TW, int PPL, int NW, bool CLAMP>
+// Stages one Gaussian for the forward: its blend terms (colours clamped at
+// zero) plus the bit mask of warp blocks its padded footprint box overlaps
+// (half-widths written by the emission kernel into r2.zw; negative means no
+// box, never cull).
+template <int TW, int PPL, int NW>
 __device__ __forceinline__ uint32_t stage_one(const float4* rec, uint32_t c, float tx0, float ty0, float4& A, float4& B,
                                               float4& Cc) {
   const float4 r0 = rec[(size_t)c * 3 + 0];
@@ -80,8 +80,7 @@ __device__ __forceinline__ uint32_t stage_one(const float4* rec, uint32_t c, flo
   const float4 r2 = rec[(size_t)c * 3 + 2];
   A = make_float4(r0.x, r0.y, r0.z, 2.f * r0.w);  // 2b is exact
   B = make_float4(r1.x, r2.y + kRejectMargin, r1.y, 0.f);
-  Cc = CLAMP ? make_float4(fmaxf(r1.z, 0.f), fmaxf(r1.w, 0.f), fmaxf(r2.x, 0.f), 0.f)
-             : make_float4(r1.z, r1.w, r2.x, 0.f);
+  Cc = make_float4(fmaxf(r1.z, 0.f), fmaxf(r1.w, 0.f), fmaxf(r2.x, 0.f), 0.f);
   const float rx = r2.z, ry = r2.w;
   if (!(rx >= 0.f) || !(ry >= 0.f)) return (1u << NW) - 1u;
   uint32_t mask = 0;
@@ -227,7 +226,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     for (uint32_t j = threadIdx.x; j < nb; j += NT) {
       const uint32_t c = vals[b0 + j] & vmask;
       float4 A, B, Cc;
-      s_mask[j] = (uint8_t)stage_one<TW, PPL, NW, true>(rec, c, tx0, ty0, A, B, Cc);
+      s_mask[j] = (uint8_t)stage_one<TW, PPL, NW>(rec, c, tx0, ty0, A, B, Cc);
       s_a[j] = A;
       s_b[j] = B;
       s_c[j] = Cc;
