@@ -39,6 +39,8 @@ def parse():
     p.add_argument("--views", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage batched timing")
+    p.add_argument("--no-precision", action="store_true", help="skip the FP64 precision report (CPU baseline leg)")
     p.add_argument("--mode", default="bench", choices=["bench", "profile"],
                    help="profile: warm up, then run exactly one non-graph batched step (for ncu launch lists)")
     return p.parse_args()
@@ -201,12 +203,34 @@ def stage_profile(ctx, fn):
     return {k: float(buf[i]) for i, k in enumerate(_lib.PROFILE_STAGES)}
 
 
-def cpu_baseline(scene, cams, targets_np):
+def _psnr(a, b):
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return float("inf") if mse == 0.0 else 10.0 * np.log10(1.0 / mse)
+
+
+def _grad_rel(g, r):
+    """Norm-wise relative error of the concatenated parameter gradients."""
+    keys = ("v_transforms", "v_sh", "v_raw_opacity")
+    gv = np.concatenate([np.asarray(g[k], np.float64).reshape(-1) for k in keys])
+    rv = np.concatenate([np.asarray(r[k], np.float64).reshape(-1) for k in keys])
+    return float(np.linalg.norm(gv - rv) / max(np.linalg.norm(rv), 1e-300))
+
+
+def cpu_baseline(scene, cams, targets_np, gpu_view=None):
     """CPU baselines on one view of the workload (a bounded sample, ~10-30 s):
     the oracle (C++ restatement of the training path, forward + loss + exact
     backward, OpenMP over all host threads) is the value; the reference's own
     shipped CPU renderer (tiled_renderer.rs restated, forward only, one
-    thread, different semantics) is reported beside it."""
+    thread, different semantics) is reported beside it.
+
+    The same oracle run anchors the precision report: with gpu_view(sh_dtype,
+    sh, v_rgba) -> (image RGBA, gradients) rendering and differentiating the
+    view on the GPU, the FP32 and BF16-storage results are compared with the
+    FP64 instantiation of the oracle (image PSNR and max |diff|, norm-wise
+    gradient relative error; for BF16 against the stored, rounded SH and
+    against the unrounded scene) and with the training target (PSNR)."""
+    import torch
+
     from oracle import oracle as O
 
     cam = cams[0]
@@ -218,12 +242,32 @@ def cpu_baseline(scene, cams, targets_np):
     t1 = time.perf_counter()
     O.ref_cpu_forward(scene, cam)
     dt_ref = time.perf_counter() - t1
-    return {"value": dt * 1000.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": "1 of the 8 views (1M Gaussians, 1280x720): oracle forward + loss + exact backward, "
-                      "OpenMP over all host threads",
-            "reference_cpu_forward": {"value": dt_ref * 1000.0, "unit": UNIT, "cores": 1,
-                                      "sample": "the same view through the reference's shipped CPU renderer "
-                                                "(TiledRenderer, forward only, single-threaded as shipped)"}}
+    out = {"value": dt * 1000.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+           "sample": "1 of the 8 views (1M Gaussians, 1280x720): oracle forward + loss + exact backward, "
+                     "OpenMP over all host threads",
+           "reference_cpu_forward": {"value": dt_ref * 1000.0, "unit": UNIT, "cores": 1,
+                                     "sample": "the same view through the reference's shipped CPU renderer "
+                                               "(TiledRenderer, forward only, single-threaded as shipped)"}}
+    if gpu_view is None:
+        return out
+    tgt = targets_np[0]
+    sh_bf = torch.as_tensor(scene.sh).to(torch.bfloat16).float().numpy()
+    prec = {"view": "view 0 of the workload; upstream gradient = the oracle's loss gradient of that view"}
+    for name, sh_gpu, sh_ref in (("f32", scene.sh, scene.sh), ("bf16_sh", scene.sh, sh_bf)):
+        img, g = gpu_view("bf16" if name == "bf16_sh" else "f32", sh_gpu, vp)
+        r64 = O.Forward(scene.transforms, sh_ref, scene.raw_opacity, scene.sh_degree, cam, f64=True)
+        g64 = r64.backward(vp.astype(np.float64), mode=0)
+        e = {"image_psnr_vs_fp64_db": _psnr(img[..., :3], r64.image[..., :3]),
+             "image_max_abs_vs_fp64": float(np.abs(img - r64.image).max()),
+             "grad_rel_err_vs_fp64": _grad_rel(g, g64),
+             "psnr_vs_target_db": _psnr(img[..., :3], tgt)}
+        if name == "bf16_sh":
+            u64 = O.Forward(scene.transforms, scene.sh, scene.raw_opacity, scene.sh_degree, cam, f64=True)
+            e["grad_rel_err_vs_fp64_unrounded_scene"] = _grad_rel(g, u64.backward(vp.astype(np.float64), mode=0))
+        prec[name] = e
+    prec["bf16_psnr_loss_vs_target_db"] = prec["f32"]["psnr_vs_target_db"] - prec["bf16_sh"]["psnr_vs_target_db"]
+    out["precision"] = prec
+    return out
 
 
 def run_reference(args):
@@ -361,6 +405,9 @@ def main():
     tr_prof.opt = trainer.opt
     stages = stage_profile(ctx, lambda: tr_prof.train_step(cams, targets, args.warmup + args.steps + 1))
     hbm, peak_kind = peaks()
+    # Gaussian-pixel evaluations of the step's forward: per pixel, the list
+    # entries up to its termination (the reference's blend loop count).
+    evals_per_step = sum(int(ctx.export(v, "nvisit").astype(np.int64).sum()) for v in range(nv))
     # Algorithmic bytes per launch (all views of the step).
     algo = {
         "raster_fwd": sum(40 * I[v] + 16 * P for v in range(nv)),
@@ -387,6 +434,18 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes": algo[dom], "launch_ms": stages[dom]}
+
+    # ---- the same batched step with BF16 SH storage ---------------------------
+    bf16_ms = None
+    if not args.no_bf16:
+        ctx_b = make_context(args.n, nv, sh_dtype="bf16", tile=tile, batch=batch)
+        splats_b = host_splats_to_device(sc, sh_dtype=torch.bfloat16)
+        fit_capacity(ctx_b, splats_b, cams)
+        trainer_b = Trainer(ctx_b, splats_b, LearningRates(), total_iterations=30000, use_graph=True)
+        bf16_ms = time_steps(lambda it: trainer_b.train_step(cams, targets, it), args.steps, args.warmup,
+                             world) / args.steps / nv
+        del trainer_b, splats_b
+        ctx_b.close()
 
     # ---- plain single-view path (one view per call, FP32, no graph) ------------
     plain = None
@@ -425,9 +484,23 @@ def main():
     e2e = {"value": ms_e2e / nv, "unit": UNIT, "h2d_bytes_per_step": int(sum(f.numel() for f in host_frames)),
            "d2h_bytes_per_step": int(nv * 4), "inputs": "8-bit RGB frames, converted to f32 targets on the device"}
 
+    def gpu_view(sh_dtype, sh, v_rgba):
+        # View 0 rendered and differentiated on the GPU from the scene's own
+        # (unstepped) parameters, for the precision report.
+        cp = make_context(args.n, 1, sh_dtype=sh_dtype, tile=tile, batch=batch)
+        sp = host_splats_to_device(S.Scene(sc.transforms, sh, sc.raw_opacity, sc.sh_degree, [cams[0]]),
+                                   sh_dtype=torch.bfloat16 if sh_dtype == "bf16" else torch.float32)
+        fit_capacity(cp, sp, [cams[0]])
+        _, imgs, _ = cp.render_forward(sp, [cams[0]])
+        g = cp.render_backward(sp, torch.as_tensor(np.ascontiguousarray(v_rgba), device="cuda"))
+        torch.cuda.synchronize()
+        res = imgs[0].cpu().numpy(), {k: g[k].cpu().numpy() for k in ("v_transforms", "v_sh", "v_raw_opacity")}
+        cp.close()
+        return res
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(sc, cams, targets.cpu().numpy())
+        cpu = cpu_baseline(sc, cams, targets.cpu().numpy(), None if args.no_precision else gpu_view)
 
     if rank == 0:
         line = {
@@ -441,6 +514,10 @@ def main():
                        "l2": "inputs larger than L2 (params 236 MB + 8 views of state per step)",
                        "visible_per_view": V, "intersections_per_view": I, "parallelism": "replicas" if world > 1 else "1 GPU"},
             "plain_single_view_ms_per_view": plain,
+            "bf16_sh_batched_ms_per_view": bf16_ms,
+            "gaussian_pixel_evals_per_step": evals_per_step,
+            "gaussian_pixel_evals_per_s": evals_per_step / (ms_step * 1e-3),
+            "precision": (cpu or {}).pop("precision", None),
             "stages_ms_per_step": stages,
             "roofline": roofline,
             "cpu_baseline": cpu,
