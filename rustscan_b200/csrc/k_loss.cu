@@ -268,11 +268,23 @@ __global__ void __launch_bounds__(kLT, 5) ssim_bwd_kernel(LossArgs a) {
   }
   __syncthreads();
   // Adjoint of the vertical pass: tile rows, all halo columns (in pairs).
+  // When every output row and its taps lie strictly inside the image (no
+  // border row, no clamped tap), each tap weighs k[R + d] and no check is
+  // needed; the sums are the same operations in the same order.
+  const bool rows_inside = y0 >= R + 1 && y0 + LTY + R <= H - 1;
   for (int i = threadIdx.x; i < LTY * (HX / 2); i += blockDim.x) {
     const int oy = i / (HX / 2), hx = 2 * (i % (HX / 2));
     const int py = y0 + oy;
     float2 acc[3] = {f2(0.f), f2(0.f), f2(0.f)};
-    if (py < H) {
+    if (rows_inside) {
+#pragma unroll
+      for (int d = -R; d <= R; ++d) {
+        const float w = a.k[R + d];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+          acc[m] = fma2(f2(w), *reinterpret_cast<const float2*>(&S.g[m][oy + R + d][hx]), acc[m]);
+      }
+    } else if (py < H) {
       const bool interior = py > 0 && py < H - 1;
 #pragma unroll
       for (int d = -R; d <= R; ++d) {
