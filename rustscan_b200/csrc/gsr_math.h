@@ -575,18 +575,20 @@ template <class F> struct Projected {
 
 // Geometric part of the projection. The quaternion is normalised by the
 // reciprocal square root of its squared norm (project_forward.wgsl:38-42).
+// The view-independent part: the 3D covariance from the normalised
+// quaternion and the scales, and the opacity (ok = false for a degenerate
+// quaternion, which no view projects).
+template <class F> struct GaussWorld {
+  M3<F> cov3d;
+  F opacity;
+  bool ok;
+};
 template <class F>
-GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, V3<F> log_scale, F raw_opac,
-                                     F cov_blur, TileShape ts, uint32_t tiles_x, uint32_t tiles_y,
-                                     bool hp = false) {
-  Projected<F> p;
-  p.visible = false;
-  const V3<F> mc = world_to_cam(cam, mean);
-  p.depth = mc.z;
-  if (mc.z < F(0.01) || mc.z > F(1e10)) return p;
+GSR_HD GaussWorld<F> gauss_world(V4<F> quat, V3<F> log_scale, F raw_opac) {
+  GaussWorld<F> w;
   const F qn = quat.x * quat.x + quat.y * quat.y + quat.z * quat.z + quat.w * quat.w;
-  if (qn < F(1e-6)) return p;
-  const F rs = F(1) / gsqrt(qn);
+  w.ok = !(qn < F(1e-6));
+  const F rs = F(1) / gsqrt(w.ok ? qn : F(1));
   quat.x = quat.x * rs;
   quat.y = quat.y * rs;
   quat.z = quat.z * rs;
@@ -595,10 +597,25 @@ GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, 
   scale.x = gexp(log_scale.x);
   scale.y = gexp(log_scale.y);
   scale.z = gexp(log_scale.z);
-  F opacity = sigmoid(raw_opac);
+  w.opacity = sigmoid(raw_opac);
   const M3<F> m = rot_scale(quat_to_mat3(quat), scale);
-  const M3<F> cov3d = mul(m, transpose(m));
-  const M3<F> cov_cam = mul(mul(cam.rot, cov3d), transpose(cam.rot));
+  w.cov3d = mul(m, transpose(m));
+  return w;
+}
+
+// project_gaussian with the view-independent part computed once (kernels
+// that project one Gaussian into many views).
+template <class F>
+GSR_HD Projected<F> project_gaussian_w(const Cam<F>& cam, V3<F> mean, const GaussWorld<F>& gw, F cov_blur,
+                                       TileShape ts, uint32_t tiles_x, uint32_t tiles_y, bool hp = false) {
+  Projected<F> p;
+  p.visible = false;
+  const V3<F> mc = world_to_cam(cam, mean);
+  p.depth = mc.z;
+  if (mc.z < F(0.01) || mc.z > F(1e10)) return p;
+  if (!gw.ok) return p;
+  F opacity = gw.opacity;
+  const M3<F> cov_cam = mul(mul(cam.rot, gw.cov3d), transpose(cam.rot));
   const M32<F> j = calc_cam_j(mc, cam);
   M2<F> cov2d = mul(mul(j, cov_cam), transpose(j));
   opacity = opacity * (hp ? compensate_cov2d_hp(cov2d, cov_blur) : compensate_cov2d(cov2d, cov_blur));
@@ -621,6 +638,13 @@ GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, 
   p.thr = thr;
   p.box = tile_bbox(mean2d, ext, ts, tiles_x, tiles_y);
   return p;
+}
+
+template <class F>
+GSR_HD Projected<F> project_gaussian(const Cam<F>& cam, V3<F> mean, V4<F> quat, V3<F> log_scale, F raw_opac,
+                                     F cov_blur, TileShape ts, uint32_t tiles_x, uint32_t tiles_y,
+                                     bool hp = false) {
+  return project_gaussian_w(cam, mean, gauss_world(quat, log_scale, raw_opac), cov_blur, ts, tiles_x, tiles_y, hp);
 }
 
 // Number of tiles of the box that pass the contribution test, visited in

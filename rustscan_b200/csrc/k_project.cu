@@ -120,12 +120,13 @@ __global__ void __launch_bounds__(kProjThreads) visibility_kernel(ProjectArgs a)
   const GaussParams q = stage_params(a.sp, g0, rows, s_tr4);
   const bool valid = threadIdx.x < rows;
   const TileShape ts{a.vs.tile_w, a.vs.tile_h};
+  const GaussWorld<float> gw = gauss_world(q.quat, q.ls, q.raw);  // once for all views
   for (uint32_t v = 0; v < nv; ++v) {
     const ViewDesc& vd = a.vs.views[v];
     const Cam<float> cam = cam_from_desc<float>(vd);
     bool vis = false;
     if (valid)
-      vis = project_gaussian(cam, q.mean, q.quat, q.ls, q.raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0)
+      vis = project_gaussian_w(cam, q.mean, gw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0)
                 .visible;
     const uint32_t m = __ballot_sync(0xffffffffu, vis);
     if (lane == 0) {
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(kProjThreads) records_kernel(ProjectArgs a) {
   __syncthreads();
   const bool valid = threadIdx.x < rows;
   const TileShape ts{a.vs.tile_w, a.vs.tile_h};
+  const GaussWorld<float> gw = gauss_world(q.quat, q.ls, q.raw);  // once for all views
   const float* shg = s_sh + threadIdx.x * ShRows<DEG>::kStride;
   for (uint32_t v = 0; v < nv; ++v) {
     const uint32_t m = s_mask[v][warp];
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(kProjThreads) records_kernel(ProjectArgs a) {
       const ViewDesc& vd = a.vs.views[v];
       const Cam<float> cam = cam_from_desc<float>(vd);
       const Projected<float> p =
-          project_gaussian(cam, q.mean, q.quat, q.ls, q.raw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
+          project_gaussian_w(cam, q.mean, gw, a.cov_blur, ts, vd.tiles_x, vd.tiles_y, a.hp != 0);
       auto coeff = [&](int k, int ch) { return shg[k * 3 + ch]; };
       const V3<float> rgb = sh_to_color<float>(DEG, view_dir(cam, q.mean), coeff);
       float4* r = slice(a.b.rec, a.b.Vcap * 3, v) + (size_t)c * 3;
