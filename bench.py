@@ -116,14 +116,17 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    cuda = torch.cuda.is_available()
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
+        if cuda:
+            torch.cuda.set_device(local)
+        # NCCL between GPUs; gloo where there is none (the host-side checks).
+        dist.init_process_group("nccl" if cuda else "gloo", timeout=datetime.timedelta(seconds=300))
+    elif cuda:
         torch.cuda.set_device(0)
     return world, rank, local
 
@@ -141,7 +144,7 @@ def max_over_ranks(world, x):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
