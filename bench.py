@@ -426,8 +426,8 @@ def main():
     # intersections), scaled to the launch by its intersections (the raster
     # and tile-sort traffic grows with them) or, for Adam, taken as is (it
     # sweeps the N parameters once per step).
-    traffic_coeff = {"raster_bwd": (37.752e6 + 0.012e6) / 6273269, "raster_fwd": (14.120e6 + 0.117e6) / 6273269,
-                     "tile_sort": (27.630e6 + 0.043e6 + 27.734e6 + 0.063e6) / 6273269}
+    traffic_coeff = {"raster_bwd": (37.736e6 + 0.016e6) / 6273269, "raster_fwd": (14.121e6 + 0.219e6) / 6273269,
+                     "tile_sort": (32.738e6 + 0.692e6 + 32.732e6 + 0.583e6) / 6273269}
     if dom in traffic_coeff:
         traffic = traffic_coeff[dom] * sum(I)
     elif dom == "adam":
