@@ -7,8 +7,9 @@
 //  - one histogram pass over the keys computes the digit counts of every
 //    radix pass at once;
 //  - each radix pass is one persistent launch: blocks take 4096-key
-//    partitions by ticket, rank keys stably inside the block (warp
-//    match_any per digit, warps in order), publish per-digit counts and look
+//    partitions by ticket, rank keys stably inside the block (peer lanes
+//    of a digit by match_any, or by one ballot per digit bit where the
+//    digits are near-random; warps in order), publish per-digit counts and look
 //    back across partitions for their global offsets, then scatter through
 //    shared memory so that every digit's run is written contiguously;
 //  - scans are single-pass with the same look-back.
@@ -88,7 +89,7 @@ struct SortPassArgs {
 
 // KV: values travel with the keys; otherwise the keys are sorted alone.
 template <bool KV>
-__global__ void __launch_bounds__(kSortThreads, KV ? 2 : 3) sort_pass_kernel(SortPassArgs a) {
+__global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(SortPassArgs a) {
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[KV ? kSortTile : 1];
   __shared__ uint32_t s_whist[kSortWarps][256];
@@ -97,6 +98,8 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 3) sort_pass_kernel(Sor
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_ticket;
   const uint32_t epoch = epoch_begin(a.ctl);
+  const unsigned long long tag = (unsigned long long)(epoch & 0x3fffffffu) << 34;
+  const int dbits = __popc(a.dmask);
   const uint32_t seg = blockIdx.y;
   const uint32_t n = seg_count(a.counts, a.count_stride, seg, a.n_host, a.cap);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -126,8 +129,26 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 3) sort_pass_kernel(Sor
     for (int i = 0; i < kSortItems; ++i) {
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       const bool ok = idx < n;
-      const uint32_t d = ok ? ((key[i] >> a.shift) & a.dmask) : (256u + lane);
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      uint32_t d, peers;
+      if (KV) {
+        // Near-random digits (depth keys): one ballot per digit bit.
+        d = (key[i] >> a.shift) & a.dmask;
+        const uint32_t okm = __ballot_sync(0xffffffffu, ok);  // every lane, also past the end
+        peers = ok ? okm : (1u << lane);
+#pragma unroll
+        for (int bit = 0; bit < 8; ++bit) {
+          if (bit < dbits) {
+            const bool set = (d >> bit) & 1u;
+            const uint32_t bb = __ballot_sync(0xffffffffu, set);
+            peers &= set ? bb : ~bb;
+          }
+        }
+      } else {
+        // Clustered digits (tile ids of neighbouring boxes): few distinct
+        // values per warp, where match_any is cheaper.
+        d = ok ? ((key[i] >> a.shift) & a.dmask) : (256u + lane);
+        peers = __match_any_sync(0xffffffffu, d);
+      }
       const uint32_t below = peers & lt_mask;
       uint32_t b = 0;
       if (ok) b = s_whist[warp][d];
@@ -146,9 +167,13 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 3) sort_pass_kernel(Sor
       s_whist[w][d] = sum;
       sum += t;
     }
+    // The digit counts are published before the block scan, so that later
+    // partitions can sum past this one as early as possible; only the
+    // pass's digits look back.
+    if (d <= a.dmask) st_volatile64(states + (size_t)part * 256 + d, tag | (part == 0 ? kFlagPre : kFlagAgg) | sum);
     uint32_t tot;
     const uint32_t dstart = block_exclusive_scan(sum, s_scan, &tot);
-    const uint32_t excl = lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort);
+    const uint32_t excl = d <= a.dmask ? lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort) : 0u;
     s_dstart[d] = dstart;
     s_gbase[d] = gbase[d] + excl - dstart;
     __syncthreads();
@@ -314,7 +339,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.parts_cap = parts_cap;
     a.ctl = s.ctl;
     a.status = s.status;
-    dim3 grid(persistent_blocks(s.num_sms, segments, 3), segments);
+    dim3 grid(persistent_blocks(s.num_sms, segments, kv ? 3 : 4), segments);
     if (kv)
       sort_pass_kernel<true><<<grid, kSortThreads, 0, st>>>(a);
     else
