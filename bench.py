@@ -427,7 +427,7 @@ def main():
     # and tile-sort traffic grows with them) or, for Adam, taken as is (it
     # sweeps the N parameters once per step).
     traffic_coeff = {"raster_bwd": (37.736e6 + 0.016e6) / 6273269, "raster_fwd": (14.121e6 + 0.219e6) / 6273269,
-                     "tile_sort": (32.738e6 + 0.692e6 + 32.732e6 + 0.583e6) / 6273269}
+                     "tile_sort": (30.3e6 + 0.4e6 + 30.4e6 + 0.6e6) / 6273269}
     if dom in traffic_coeff:
         traffic = traffic_coeff[dom] * sum(I)
     elif dom == "adam":
