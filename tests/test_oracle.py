@@ -301,3 +301,63 @@ def test_topology_known_answers():
                                train_t=0.5)
     np.testing.assert_allclose(np.exp(t[0, 7]), 0.09, atol=1e-6)
     np.testing.assert_allclose(1 / (1 + np.exp(-o[0])), 0.45, atol=1e-6)
+
+
+def _tile_test(tx, ty, tw, th, mx, my, cx, cy, cz, thr):
+    """helpers.wgsl:237-283 (will_primitive_contribute) restated with Python
+    floats (IEEE doubles, every operation rounded, in the expression order of
+    the WGSL), for the FP64 oracle."""
+    rx0, ry0 = float(tx * tw), float(ty * th)
+    rx1, ry1 = rx0 + float(tw), ry0 + float(th)
+    x_left, x_right = mx < rx0, mx > rx1
+    y_above, y_below = my < ry0, my > ry1
+    in_x, in_y = not (x_left or x_right), not (y_above or y_below)
+    if in_x and in_y:
+        return True
+    ccx = rx0 if x_left else rx1
+    ccy = ry0 if y_above else ry1
+    dxv = (rx1 - rx0) if x_left else -(rx1 - rx0)
+    dyv = (ry1 - ry0) if y_above else -(ry1 - ry0)
+    diffx, diffy = mx - ccx, my - ccy
+    tmx = tmy = 0.0
+    if not in_y:
+        tmx = min(max((dxv * cx * diffx + dxv * cy * diffy) / max(dxv * cx * dxv, 1e-12), 0.0), 1.0)
+    if not in_x:
+        tmy = min(max((dyv * cy * diffx + dyv * cz * diffy) / max(dyv * cz * dyv, 1e-12), 0.0), 1.0)
+    dx, dy = (ccx + tmx * dxv) - mx, (ccy + tmy * dyv) - my
+    return 0.5 * (cx * dx * dx + 2.0 * cy * dx * dy + cz * dy * dy) <= thr
+
+
+@pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
+def test_binning_contract_matches_independent_restatement(tile):
+    """The oracle's binning against a restatement of its contract: depth
+    order with ties by global id (sorting.rs:34-61), one intersection per box
+    tile that passes the tile test, intersections ordered by (tile, depth
+    rank), and [start, end) tile ranges (get_tile_offsets.wgsl:11-30)."""
+    sc = S.small_scene(n=400, degree=1, width=96, height=72, seed=5, logscale_mu=-2.0)
+    cam = sc.cameras[0]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 1, cam, tile=tile, f64=True)
+    V, tw, th = f.num_visible, tile[0], tile[1]
+    assert V > 100
+    expected_order = sorted(range(V), key=lambda c: (float(f.depth[c]), int(f.gid[c])))
+    np.testing.assert_array_equal(f.order, expected_order)
+    rank = np.empty(V, np.int64)
+    rank[f.order] = np.arange(V)
+    pairs = []
+    for c in range(V):
+        x0, y0, x1, y1 = (int(b) for b in f.box[c])
+        mx, my, cx, cy, cz, _, thr = (float(r) for r in f.rec[c, :7])
+        passing = [(ty * f.tiles_x + tx, int(rank[c]), c) for ty in range(y0, y1) for tx in range(x0, x1)
+                   if _tile_test(tx, ty, tw, th, mx, my, cx, cy, cz, thr)]
+        assert f.count[c] == len(passing), c
+        pairs += passing
+    pairs.sort()
+    assert f.num_intersections == len(pairs) > V
+    box_tiles = sum(max(int(b[2]) - int(b[0]), 0) * max(int(b[3]) - int(b[1]), 0) for b in f.box)
+    assert box_tiles > 1.05 * len(pairs)  # the tile test rejects a share of the box tiles
+    np.testing.assert_array_equal(f.isect_tile, [p[0] for p in pairs])
+    np.testing.assert_array_equal(f.isect_c, [p[2] for p in pairs])
+    for t in range(f.tiles_x * f.tiles_y):
+        idx = np.nonzero(f.isect_tile == t)[0]
+        want = (idx[0], idx[-1] + 1) if idx.size else (0, 0)
+        assert tuple(int(r) for r in f.ranges[2 * t:2 * t + 2]) == want, t
