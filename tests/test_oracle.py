@@ -1,7 +1,8 @@
-"""CPU checks of the oracle itself: the reference's own known answers, an
-independent numpy restatement of the projection, the portable exp/log, FP64
-finite differences of the exact adjoint, and agreement of the reverse-walk
-reference mode with the literal WGSL backward walk."""
+"""CPU checks of the oracle itself: the reference's own known answers,
+independent restatements of the projection, the binning contract and the
+front-to-back blend, the portable exp/log, FP64 finite differences of the
+exact adjoint, and agreement of the reverse-walk reference mode with the
+literal WGSL backward walk."""
 import json
 import math
 import os
@@ -361,3 +362,55 @@ def test_binning_contract_matches_independent_restatement(tile):
         idx = np.nonzero(f.isect_tile == t)[0]
         want = (idx[0], idx[-1] + 1) if idx.size else (0, 0)
         assert tuple(int(r) for r in f.ranges[2 * t:2 * t + 2]) == want, t
+
+
+def _fma(a, b, c):
+    """Fused multiply-add of doubles, rounded once (exact rational arithmetic)."""
+    from fractions import Fraction
+    return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def test_forward_blend_matches_independent_restatement():
+    """The FP64 oracle's front-to-back blend against a restatement of
+    rasterize.wgsl:257-276 per pixel: sigma in the WGSL operation order,
+    alpha = min(0.999, opacity * exp(-sigma)) taken when sigma >= 0 and
+    alpha >= 1/255, colour += max(c, 0) * alpha * T as one fused multiply-add,
+    T *= 1 - alpha, stop once T < 1e-4. Every output is compared bit for bit."""
+    sc = S.small_scene(n=250, degree=1, width=64, height=48, seed=9, logscale_mu=-2.0)
+    cam = sc.cameras[0]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 1, cam, f64=True)
+    tw, th = f.tile
+    W, H = cam.width, cam.height
+    hits = f.hit_blocks()
+    want_hits = np.zeros_like(hits)
+    contributors = 0
+    for py in range(H):
+        for px in range(W):
+            tx, ty = px // tw, py // th
+            t = ty * f.tiles_x + tx
+            s0, s1 = int(f.ranges[2 * t]), int(f.ranges[2 * t + 1])
+            pcx, pcy = px + 0.5, py + 0.5
+            T, C = 1.0, [0.0, 0.0, 0.0]
+            last = nc = nv = 0
+            for s in range(s0, s1):
+                c = int(f.isect_c[s])
+                mx, my, ca, cb, cc, op = (float(v) for v in f.rec[c, :6])
+                nv += 1
+                dx, dy = mx - pcx, my - pcy
+                sigma = 0.5 * ((ca * dx * dx + 2.0 * cb * dx * dy) + cc * dy * dy)
+                alpha = min(0.999, op * math.exp(-sigma))
+                if not (sigma >= 0.0 and alpha >= 1.0 / 255.0):
+                    continue
+                vis = alpha * T
+                C = [_fma(max(float(f.rec[c, 7 + k]), 0.0), vis, C[k]) for k in range(3)]
+                T = T * (1.0 - alpha)
+                want_hits[s] |= 1 << ((px % tw) // 8 + ((py % th) // 8) * ((tw + 7) // 8))
+                last, nc = s + 1, nc + 1
+                contributors += 1
+                if T < 1e-4:
+                    break
+            assert f.image[py, px, :3].tolist() == C, (px, py)
+            assert f.image[py, px, 3] == 1.0 - T and f.tfinal[py, px] == T, (px, py)
+            assert (f.last[py, px], f.ncontrib[py, px], f.nvisit[py, px]) == (last, nc, nv), (px, py)
+    assert contributors > W * H
+    np.testing.assert_array_equal(hits, want_hits)
