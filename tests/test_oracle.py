@@ -414,3 +414,44 @@ def test_forward_blend_matches_independent_restatement():
             assert (f.last[py, px], f.ncontrib[py, px], f.nvisit[py, px]) == (last, nc, nv), (px, py)
     assert contributors > W * H
     np.testing.assert_array_equal(hits, want_hits)
+
+
+def _numpy_loss(pred, tgt, l1_weight=0.8, ssim_weight=0.2):
+    """engine/loss.rs:42-76, 112-142 (default settings) restated with numpy:
+    an 11-tap sigma-1.5 normalised Gaussian window applied separably with
+    replicate padding, C1 = 1e-4, C2 = 9e-4, both denominator factors clamped
+    at 1e-8; loss = w1 * mean |x - y| + ws * (1 - mean SSIM)."""
+    x, y = pred[..., :3], tgt
+    # loss.rs:233-250: the window values are computed in f64, stored as f32
+    # and normalised in f32 (sequential f32 sum).
+    vals = np.exp(-((np.arange(11) - 5.0) ** 2) / (2 * 1.5 ** 2)).astype(np.float32)
+    total = np.float32(0)
+    for v in vals:
+        total = np.float32(total + v)
+    k = (vals / max(total, np.float32(1e-8))).astype(np.float32).astype(np.float64)
+
+    def blur(a):
+        p = np.pad(a, 5, mode="edge")
+        h = sum(k[t] * p[:, t:t + a.shape[1]] for t in range(11))
+        return sum(k[t] * h[t:t + a.shape[0], :] for t in range(11))
+
+    maps = []
+    for c in range(3):
+        X, Y = x[..., c], y[..., c]
+        mx, my = blur(X), blur(Y)
+        sxx, syy, sxy = blur(X * X) - mx * mx, blur(Y * Y) - my * my, blur(X * Y) - mx * my
+        num = (2 * mx * my + 1e-4) * (2 * sxy + 9e-4)
+        den = np.maximum(mx * mx + my * my + 1e-4, 1e-8) * np.maximum(sxx + syy + 9e-4, 1e-8)
+        maps.append(num / den)
+    return l1_weight * np.abs(x - y).mean() + ssim_weight * (1.0 - np.mean(maps))
+
+
+@pytest.mark.parametrize("shape", [(20, 24), (37, 53), (8, 5)])
+def test_loss_value_matches_independent_numpy(shape):
+    rng = np.random.default_rng(11)
+    H, W = shape
+    pred = rng.uniform(0, 1, (H, W, 4))
+    tgt = np.clip(pred[..., :3] + rng.normal(0, 0.1, (H, W, 3)), 0, 1)
+    for w1, ws in ((0.8, 0.2), (1.0, 0.0), (0.0, 1.0)):
+        val, _ = O.loss(pred, tgt, l1_weight=w1, ssim_weight=ws, f64=True)
+        assert abs(val - _numpy_loss(pred, tgt, w1, ws)) <= 1e-12 * max(1.0, abs(val)), (shape, w1, ws)
