@@ -1,8 +1,8 @@
 """CPU checks of the oracle itself: the reference's own known answers,
-independent restatements of the projection, the binning contract and the
-front-to-back blend, the portable exp/log, FP64 finite differences of the
-exact adjoint, and agreement of the reverse-walk reference mode with the
-literal WGSL backward walk."""
+independent restatements of the projection, the binning contract, the
+front-to-back blend, the loss value, Adam and the densification sums, the
+portable exp/log, FP64 finite differences of the exact adjoint, and agreement
+of the reverse-walk reference mode with the literal WGSL backward walk."""
 import json
 import math
 import os
@@ -455,3 +455,30 @@ def test_loss_value_matches_independent_numpy(shape):
     for w1, ws in ((0.8, 0.2), (1.0, 0.0), (0.0, 1.0)):
         val, _ = O.loss(pred, tgt, l1_weight=w1, ssim_weight=ws, f64=True)
         assert abs(val - _numpy_loss(pred, tgt, w1, ws)) <= 1e-12 * max(1.0, abs(val)), (shape, w1, ws)
+
+
+@pytest.mark.parametrize("use_visible", [False, True])
+def test_densify_matches_numpy_restatement(use_visible):
+    """engine/trainer.rs:651-728 restated in float32 numpy, accumulating into
+    existing sums: grad_2d, screen_grad_2d, abs_grad_2d, abs_pixel_grad_2d,
+    pixel_coverage, camera_depth, grad_color, num_observations,
+    visible_observations."""
+    rng = np.random.default_rng(12)
+    n, K = 300, 16
+    v_tr = rng.standard_normal((n, 10)).astype(np.float32)
+    stats = rng.standard_normal((n, 7)).astype(np.float32)
+    v_sh = rng.standard_normal((n, K, 3)).astype(np.float32)
+    visible = (rng.uniform(size=n) < 0.6).astype(np.float32)
+    acc0 = rng.uniform(0, 2, (9, n)).astype(np.float32)
+    acc = acc0.copy()
+    O.densify(v_tr, stats, v_sh, visible, acc, use_visible=use_visible)
+    f3 = np.float32(3)
+    g2 = (np.abs(v_tr[:, 0]) + np.abs(v_tr[:, 1]) + np.abs(v_tr[:, 2])) / f3
+    gc = np.zeros(n, np.float32)
+    for k in range(K):
+        gc = gc + (np.abs(v_sh[:, k, 0]) + np.abs(v_sh[:, k, 1]) + np.abs(v_sh[:, k, 2])) / f3
+    gc = gc / np.float32(K)
+    add = [g2, np.sqrt(stats[:, 0] * stats[:, 0] + stats[:, 1] * stats[:, 1]),
+           np.sqrt(stats[:, 2] * stats[:, 2] + stats[:, 3] * stats[:, 3]), stats[:, 4], stats[:, 5], stats[:, 6], gc,
+           np.ones(n, np.float32), visible if use_visible else np.ones(n, np.float32)]
+    np.testing.assert_array_equal(acc, np.stack([acc0[i] + add[i] for i in range(9)]))
