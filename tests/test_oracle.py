@@ -1,5 +1,6 @@
 """CPU checks of the oracle itself: the reference's own known answers,
-independent restatements of the projection, the binning contract, the
+independent restatements of the projection, the SH colour, the binning
+contract, the
 front-to-back blend, the loss value, Adam and the densification sums, the
 portable exp/log, FP64 finite differences of the exact adjoint, and agreement
 of the reverse-walk reference mode with the literal WGSL backward walk."""
@@ -482,3 +483,41 @@ def test_densify_matches_numpy_restatement(use_visible):
            np.sqrt(stats[:, 2] * stats[:, 2] + stats[:, 3] * stats[:, 3]), stats[:, 4], stats[:, 5], stats[:, 6], gc,
            np.ones(n, np.float32), visible if use_visible else np.ones(n, np.float32)]
     np.testing.assert_array_equal(acc, np.stack([acc0[i] + add[i] for i in range(9)]))
+
+
+def _standard_sh_color(degree, d, sh):
+    """Colour of real spherical harmonics up to degree 3 in the usual 3DGS
+    convention (published constants of the real SH basis, written out term by
+    term), plus 0.5. d is a unit view direction, sh is [K, 3]."""
+    x, y, z = d
+    b = [0.28209479177387814]
+    if degree >= 1:
+        c1 = 0.4886025119029199
+        b += [-c1 * y, c1 * z, -c1 * x]
+    if degree >= 2:
+        xx, yy, zz = x * x, y * y, z * z
+        b += [1.0925484305920792 * x * y, -1.0925484305920792 * y * z,
+              0.31539156525252005 * (2 * zz - xx - yy), -1.0925484305920792 * x * z,
+              0.5462742152960396 * (xx - yy)]
+    if degree >= 3:
+        b += [-0.5900435899266435 * y * (3 * xx - yy), 2.890611442640554 * x * y * z,
+              -0.4570457994644658 * y * (4 * zz - xx - yy), 0.3731763325901154 * z * (2 * zz - 3 * xx - 3 * yy),
+              -0.4570457994644658 * x * (4 * zz - xx - yy), 1.445305721320277 * z * (xx - yy),
+              -0.5900435899266435 * x * (xx - 3 * yy)]
+    return np.asarray(b) @ sh + 0.5
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_sh_colour_matches_standard_real_sh(degree):
+    """project_visible.wgsl:141-224 evaluates the basis in a factored form;
+    the oracle's colours (FP64) against the textbook terms."""
+    sc = S.small_scene(n=300, degree=degree, width=80, height=60, seed=4, logscale_mu=-2.5)
+    cam = sc.cameras[0]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, degree, cam, f64=True)
+    assert f.num_visible > 50
+    campos = cam.campos.astype(np.float64)
+    for c, g in enumerate(f.gid):
+        d = sc.transforms[g, :3].astype(np.float64) - campos
+        d /= np.linalg.norm(d)
+        want = _standard_sh_color(degree, d, sc.sh[g].astype(np.float64))
+        np.testing.assert_allclose(f.rec[c, 7:10], want, rtol=1e-12, atol=1e-13)
