@@ -1,9 +1,9 @@
 """CPU checks of the oracle itself: the reference's own known answers,
 independent restatements of the projection, the SH colour, the binning
-contract, the
-front-to-back blend, the loss value, Adam and the densification sums, the
-portable exp/log, FP64 finite differences of the exact adjoint, and agreement
-of the reverse-walk reference mode with the literal WGSL backward walk."""
+contract, the front-to-back blend, the loss value, Adam and the densification
+sums, the portable exp/log, FP64 finite differences of the exact adjoint, and
+agreement of the reverse-walk reference mode with the literal WGSL backward
+walk."""
 import json
 import math
 import os
