@@ -140,10 +140,16 @@ GSR_API gsr_status gsr_prefix_sum_u32(gsr_ctx* ctx, const uint32_t* in, uint32_t
  *    variable) that every GPU loading the library keeps until process exit.
  *  - The first call on each device looks up that array's device address
  *    (cudaGetSymbolAddress) with the device current; make that first call
- *    before any stream capture.
- *  - All calls on a device share the one array: calls whose work overlaps
- *    on the GPU (different streams, or threads) race and give wrong results.
- *    Serialise them, e.g. on one stream.
+ *    before any stream capture. The address is cached with the ID of the
+ *    context it was found in and looked up again when the calling thread's
+ *    current context differs (after cudaDeviceReset, or under a context
+ *    other than the device's primary one); make the first call in each new
+ *    context before any stream capture as well.
+ *  - All calls on a device share the one array: the look-back states, the
+ *    launch-epoch control block and the status words that each call clears
+ *    first. Calls whose work overlaps on the GPU (different streams, or
+ *    threads) race on all of them and give wrong results. Serialise them,
+ *    e.g. on one stream.
  *  - It only enqueues work; a device-side wait that gives up cannot be
  *    reported here (results are then wrong but the call still finishes).
  * in and out are device pointers and may not alias. */
@@ -174,7 +180,7 @@ GSR_API gsr_status gsr_render_forward(gsr_ctx* ctx, const gsr_splats* splats, co
 /* Backward of the last forward for upstream image gradients v_rgba (same
  * layout as out_rgba). Writes the parameter gradients of the sum over views
  * (rows of Gaussians no view sees are zero) and, if stats is not NULL, the
- * [n_views, n, 7] densification statistics (project_backwards.wgsl:192-277).
+ * [n_views, n, 7] densification statistics (project_backwards.wgsl:33-36, 105-108).
  * Replaces RenderBackward::backward (RustGS/src/training/backward/autodiff.rs:82-142)
  * and, below it, RasterizeBwdBackend (rasterize_bwd.rs:41-54) and
  * ProjectBwdBackend (project_bwd.rs:44-52). */

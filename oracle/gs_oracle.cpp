@@ -140,7 +140,7 @@ template <class F> void forward(FwdState<F>& st) {
     const int g = st.gid_of_c[c];
     st.proj[c] = all[g];
     st.count[c] = cnt[g];
-    // project_visible.wgsl:265-305: SH colour for the visible Gaussian.
+    // project_visible.wgsl:168-208: SH colour for the visible Gaussian.
     const F* t = sp.transforms + (size_t)g * 10;
     V3<F> mean{t[0], t[1], t[2]};
     const F* shg = sp.sh + (size_t)g * sp.K * 3;
@@ -379,7 +379,7 @@ template <class F> void raster_backward(const FwdState<F>& st, const F* v_rgba, 
   }
 }
 
-// project_backwards.wgsl:182-319 for every visible Gaussian; rows of
+// project_backwards.wgsl:12-151 for every visible Gaussian; rows of
 // non-visible Gaussians stay zero (project_bwd.rs zero-fills).
 template <class F>
 void project_backward_all(const FwdState<F>& st, const BwdOut<F>& bo, bool exact, F* v_tr, F* v_sh, F* v_op,
@@ -426,7 +426,7 @@ void project_backward_all(const FwdState<F>& st, const BwdOut<F>& bo, bool exact
     o[8] = pg.v_log_scale.y;
     o[9] = pg.v_log_scale.z;
     v_op[g] = pg.v_raw_opac;
-    // project_backwards.wgsl:192-205, 274-277.
+    // project_backwards.wgsl:33-36, 105-108.
     F* s = stats + (size_t)g * 7;
     s[0] = sg.v_xy[0];
     s[1] = sg.v_xy[1];

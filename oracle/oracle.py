@@ -170,8 +170,12 @@ class Forward:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            getattr(lib(), f"orc_free_{self.suf}")(self._h)
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            try:
+                getattr(_lib, f"orc_free_{self.suf}")(h)
+            except TypeError:  # interpreter shutdown: ctypes already torn down
+                pass
             self._h = None
 
 

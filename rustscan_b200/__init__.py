@@ -361,28 +361,72 @@ def render_splats_with_visibility(ctx: Context, splats: DeviceSplats, camera: Ca
     return RenderSplatsOutput(img, vis, stats_leaf)
 
 
+_LIBM = None
+
+
+def _libm():
+    """The C library's single-precision logf/expf, which Rust's f32::ln and
+    f32::exp call on Linux."""
+    global _LIBM
+    if _LIBM is None:
+        import ctypes.util
+
+        m = C.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+        for fn in (m.logf, m.expf):
+            fn.argtypes = [C.c_float]
+            fn.restype = C.c_float
+        _LIBM = m
+    return _LIBM
+
+
+def lr_at(initial: float, final_value: float, iteration: int, iterations: int, decay_iterations=None) -> float:
+    """WgpuTrainer::lr_at (engine/trainer.rs:179-191) in f32: constant when
+    final_value <= 0, final_value >= initial or iterations == 0, else
+    initial * exp(ln(final / initial) * t) with t = min(iteration, d) / d,
+    d = decay_iterations (default: iterations), every operation rounded to
+    f32 as the reference computes it."""
+    f32 = np.float32
+    initial, final_value = f32(initial), f32(final_value)
+    if final_value <= 0 or final_value >= initial or iterations == 0:
+        return float(initial)
+    d = max(int(decay_iterations if decay_iterations is not None else iterations), 1)
+    t = f32(min(int(iteration), d)) / f32(d)
+    m = _libm()
+    ratio = f32(final_value / initial)
+    e = f32(m.expf(float(f32(f32(m.logf(float(ratio))) * t))))
+    return float(f32(initial * e))
+
+
 @dataclasses.dataclass
 class LearningRates:
-    """TrainingOptimizerConfig defaults (RustGS/src/training/config.rs:532-546)."""
+    """TrainingOptimizerConfig defaults (RustGS/src/training/config.rs:532-546):
+    every group has an initial rate and a final rate (0: constant) with the
+    exponential schedule of lr_at; only the position rate decays by default."""
 
     position: float = 0.00016
     position_final: float = 0.0000016
     rotation: float = 0.001
+    rotation_final: float = 0.0
     scale: float = 0.005
+    scale_final: float = 0.0
     color: float = 0.0025
+    color_final: float = 0.0
     opacity: float = 0.05
+    opacity_final: float = 0.0
+    decay_iterations: int | None = None
     beta1: float = 0.9
     beta2: float = 0.999
     eps: float = 1e-8
 
     def at(self, iteration, total):
-        """Exponential position decay (engine/trainer.rs:179-195); the others stay constant."""
-        pos = self.position
-        if 0 < self.position_final < self.position and total > 0:
-            t = min(iteration, total) / total
-            pos = self.position * math.exp(math.log(self.position_final / self.position) * t)
+        """The rates of WgpuTrainer::update_optimizer_lrs (engine/trainer.rs:221-250)
+        at `iteration` of `total` training iterations."""
         lr = _lib.gsr_lr()
-        lr.position, lr.rotation, lr.scale, lr.color, lr.opacity = pos, self.rotation, self.scale, self.color, self.opacity
+        lr.position = lr_at(self.position, self.position_final, iteration, total, self.decay_iterations)
+        lr.rotation = lr_at(self.rotation, self.rotation_final, iteration, total, self.decay_iterations)
+        lr.scale = lr_at(self.scale, self.scale_final, iteration, total, self.decay_iterations)
+        lr.color = lr_at(self.color, self.color_final, iteration, total, self.decay_iterations)
+        lr.opacity = lr_at(self.opacity, self.opacity_final, iteration, total, self.decay_iterations)
         lr.beta1, lr.beta2, lr.eps = self.beta1, self.beta2, self.eps
         return lr
 
@@ -531,6 +575,7 @@ class Trainer:
             self.loss = torch.zeros(len(cams), dtype=torch.float32, device="cuda")
         self.opt.step += 1
         p = _lib.gsr_train_params()
+        # WgpuTrainer::train_step passes iteration.saturating_sub(1) (engine/trainer.rs:362-365).
         p.lr = self.opt.lrs.at(max(iteration - 1, 0), self.total)
         p.step = self.opt.step
         p.l1_weight, p.ssim_weight = self.l1_weight, self.ssim_weight

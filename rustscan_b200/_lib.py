@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgsr.so")
 
 GSR_OK = 0
+GSR_ERR_INVALID_ARG = 1
 STATUS_NAMES = {
     0: "GSR_OK",
     1: "GSR_ERR_INVALID_ARG",

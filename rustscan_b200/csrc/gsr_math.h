@@ -389,7 +389,7 @@ GSR_HD TileBox tile_bbox(V2<F> center, V2<F> ext, TileShape ts, uint32_t tiles_x
   return b;
 }
 
-// helpers.wgsl:232-235 (forward form, also used by rasterize.wgsl:259-263):
+// helpers.wgsl:232-235 (forward form, also used by rasterize.wgsl:67-72):
 // 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with delta = point - mean.
 template <class F> GSR_HD F calc_sigma(F px, F py, V3<F> conic, V2<F> mean) {
   const F dx = px - mean.x, dy = py - mean.y;
@@ -424,7 +424,7 @@ GSR_HD bool will_primitive_contribute(uint32_t tx, uint32_t ty, TileShape ts, V2
 }
 
 // ----------------------------------------------------------------------------
-// Spherical harmonics (project_visible.wgsl:141-224 and helpers.wgsl:289-380).
+// Spherical harmonics (project_visible.wgsl:44-127 and helpers.wgsl:289-380).
 // ----------------------------------------------------------------------------
 GSR_HD constexpr int num_sh_coeffs(int degree) { return (degree + 1) * (degree + 1); }
 
@@ -481,7 +481,7 @@ template <class S> GSR_HD void sh_basis(int degree, S x, S y, S z, S* b) {
 }
 
 // Colour = sum_k b_k * coeff_k, accumulated band by band in the WGSL order
-// (project_visible.wgsl:141-224), then + 0.5 (project_visible.wgsl:305).
+// (project_visible.wgsl:44-127), then + 0.5 (project_visible.wgsl:208).
 // coeff(k, ch) is a functor returning the coefficient as F.
 template <class F, class Coeff> GSR_HD V3<F> sh_to_color(int degree, V3<F> dir, const Coeff& coeff) {
   F b[25] = {};
@@ -561,7 +561,7 @@ template <class F> GSR_HD void sh_basis_grad(int degree, V3<F> dir, F* b, F (*db
 
 // ----------------------------------------------------------------------------
 // Projection of one Gaussian (project_forward.wgsl:19-96 and
-// project_visible.wgsl:233-310, computed once).
+// project_visible.wgsl:130-214, computed once).
 // ----------------------------------------------------------------------------
 template <class F> struct Projected {
   bool visible;
@@ -657,7 +657,7 @@ template <class F> GSR_HD uint32_t count_tiles(const Projected<F>& p, TileShape 
   return n;
 }
 
-// View direction for SH (project_visible.wgsl:265-266).
+// View direction for SH (project_visible.wgsl:168-169).
 template <class F> GSR_HD V3<F> view_dir(const Cam<F>& cam, V3<F> mean) {
   V3<F> d;
   d.x = mean.x - cam.campos.x;
@@ -672,7 +672,7 @@ template <class F> GSR_HD V3<F> view_dir(const Cam<F>& cam, V3<F> mean) {
 }
 
 // ----------------------------------------------------------------------------
-// Per-pixel blend step (rasterize.wgsl:257-276).
+// Per-pixel blend step (rasterize.wgsl:65-85).
 // ----------------------------------------------------------------------------
 // sigma = 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with d = mean - pixel centre,
 // each operation rounded on its own. blend_sigma_shared takes the two
@@ -902,7 +902,7 @@ template <class F> struct SplatGrad {
   F count;
 };
 
-// Parameter gradients of one Gaussian (project_backwards.wgsl:188-319).
+// Parameter gradients of one Gaussian (project_backwards.wgsl:51-151).
 template <class F> struct ParamGrad {
   V3<F> v_mean;
   V4<F> v_quat;

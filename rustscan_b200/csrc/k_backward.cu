@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kGT, DEG >= 4 ? 2 : 4) gather_kernel(GatherArg
         // Densification quantities of this view (engine/trainer.rs:660-727).
         g2d = (fabsf(vm.x) + fabsf(vm.y) + fabsf(vm.z)) / 3.0f;
         gcol = csum * (1.0f / (float)(3 * K));  // mean over coefficients of the channel mean
-        // project_backwards.wgsl:192-205, 274-277.
+        // project_backwards.wgsl:33-36, 105-108.
         st[0] = q5.x;
         st[1] = q5.y;
         st[2] = q5.z;

@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256) ranges_kernel(FwdBufs b) {
 }
 
 // visible[v][gid] = 1 for Gaussians that contributed to a pixel of view v
-// (the `visible` output of rasterize.wgsl:270). out must be zeroed.
+// (the `visible` output of rasterize.wgsl:79). out must be zeroed.
 __global__ void __launch_bounds__(256) visible_kernel(FwdBufs b, uint32_t n, float* out) {
   const uint32_t v = blockIdx.y;
   const uint32_t V = b.vcount[v * 4 + 0];

@@ -1,7 +1,7 @@
 // k_project.cu — projection, SH colour, tile counting and compaction.
 //
 // Three passes over every Gaussian and every view of the launch
-// (project_forward.wgsl:19-96, project_visible.wgsl:233-310):
+// (project_forward.wgsl:19-96, project_visible.wgsl:130-214):
 //  1. visibility: one thread per Gaussian projects it in every view and
 //     records warp ballot words and per-block visible counts (the block
 //     stages its 256 x 40-byte transform rows with 128-bit loads);

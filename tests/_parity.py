@@ -1,8 +1,28 @@
 """Shared helpers of the parity tests: run a scene through the C ABI and
-through the CPU oracle, and compare."""
+through the CPU oracle, and compare.
+
+With GSR_PARITY_REPORT set to a file path, every gradient comparison
+appends one JSON line to it (test id, quantity, norm-wise relative error
+against the FP32 and FP64 oracles, the FP32 oracle's own error, and the
+per-element 50th/99th-percentile and maximum relative errors against FP64),
+so a run leaves the measured errors beside its pass/fail verdicts."""
+import json
+import os
+
 import numpy as np
 
 from oracle import oracle as O
+
+
+def report(what, **metrics):
+    """Append one measurement to $GSR_PARITY_REPORT (no-op when unset)."""
+    path = os.environ.get("GSR_PARITY_REPORT")
+    if not path:
+        return
+    rec = {"test": os.environ.get("PYTEST_CURRENT_TEST", "").split(" ")[0], "what": what}
+    rec.update({k: (float(v) if isinstance(v, (np.floating, float)) else v) for k, v in metrics.items()})
+    with open(path, "a") as fh:
+        fh.write(json.dumps(rec) + "\n")
 
 
 def run_gpu_forward(ctx, splats, cams):
@@ -108,6 +128,16 @@ def assert_grad_parity(g, r32, r64, rtol=1e-4, floor_frac=1e-3, what=""):
     g = np.asarray(g, np.float64)
     r32 = np.asarray(r32, np.float64)
     r64 = np.asarray(r64, np.float64)
+    if g.size:
+        e_el = rel_err(g, r64, floor_frac)
+        e_or = rel_err(r32, r64, floor_frac)
+        n64 = max(float(np.linalg.norm(r64)), 1e-300)
+        report(what, n=int(g.size),
+               norm_rel_vs_fp32=float(np.linalg.norm(g - r32)) / max(float(np.linalg.norm(r32)), 1e-300),
+               norm_rel_vs_fp64=float(np.linalg.norm(g - r64)) / n64,
+               oracle_fp32_norm_rel_vs_fp64=float(np.linalg.norm(r32 - r64)) / n64,
+               elem_rel_vs_fp64_p50=float(np.quantile(e_el, 0.5)), elem_rel_vs_fp64_p99=float(np.quantile(e_el, 0.99)),
+               elem_rel_vs_fp64_max=float(e_el.max()), oracle_fp32_elem_rel_p99=float(np.quantile(e_or, 0.99)))
     nrm = float(np.linalg.norm(r32))
     if nrm > 0:
         ne = float(np.linalg.norm(g - r32)) / nrm

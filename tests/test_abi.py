@@ -94,3 +94,47 @@ def test_context_refuses_without_gpu():
 
     with pytest.raises(RuntimeError):
         Context(max_splats=16)
+
+
+def _header_signatures():
+    """{function: argument count} and {struct: [field names]} from include/gsr.h."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    funcs = {}
+    for name, args in re.findall(r"\b(gsr_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        a = args.strip()
+        funcs[name] = 0 if a in ("", "void") else a.count(",") + 1
+    structs = {}
+    for body, name in re.findall(r"typedef struct \w+\s*\{(.*?)\}\s*(\w+)\s*;", text, flags=re.S):
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            # "uint32_t tile_w, tile_h" declares two fields; arrays keep their name.
+            head, *rest = decl.split(",")
+            fields.append(re.findall(r"(\w+)\s*(?:\[[^\]]*\])?\s*$", head)[0])
+            fields += [re.sub(r"\[.*", "", r).strip().lstrip("*") for r in rest]
+        structs[name] = fields
+    return funcs, structs
+
+
+def test_integration_rust_binding_matches_header():
+    """INTEGRATION.md's gsr-sys block declares every function of the header
+    with the same number of arguments, and every structure with the same
+    fields in the same order."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = re.search(r"```rust\n(.*?)```", doc, flags=re.S).group(1)
+    funcs, structs = _header_signatures()
+    rust_funcs = {}
+    for name, args in re.findall(r"pub fn (gsr_\w+)\s*\((.*?)\)\s*(?:->[^;]*)?;", block, flags=re.S):
+        a = args.strip().rstrip(",")
+        rust_funcs[name] = 0 if not a else a.count(":")
+    assert sorted(rust_funcs) == sorted(funcs), set(rust_funcs) ^ set(funcs)
+    for name, n in funcs.items():
+        assert rust_funcs[name] == n, (name, rust_funcs[name], n)
+    rust_structs = {}
+    for name, body in re.findall(r"pub struct (gsr_\w+)\s*\{(.*?)\}", block, flags=re.S):
+        rust_structs[name] = re.findall(r"pub (\w+)\s*:", body)
+    for name, fields in structs.items():
+        assert name in rust_structs, name
+        assert rust_structs[name] == fields, (name, rust_structs[name], fields)

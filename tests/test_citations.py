@@ -1,0 +1,68 @@
+"""Every line citation of a reference file in this repository points inside
+that file: `name.wgsl:N`, `name.wgsl:A-B` (and comma lists of those) for the
+shaders, and the same for Rust sources cited by a path whose last components
+identify one file of the reference (`engine/trainer.rs:179-191`). Runs when
+the RustScan checkout is at hand (RUSTSCAN_REFERENCE, default
+/root/reference) and skips otherwise."""
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.environ.get("RUSTSCAN_REFERENCE", "/root/reference")
+# Files written by the build's reviewers and surveyors, not by this repository.
+SKIP_FILES = {"VERDICT.md", "SURVEY.md", "ADVICE.md", "BASELINE.md"}
+CITE = re.compile(r"((?:[A-Za-z0-9_]+/)*[A-Za-z0-9_]+\.(?:wgsl|rs)):(\d+(?:-\d+)?(?:,\s?\d+(?:-\d+)?)*)")
+
+
+def _reference_files():
+    files = {}
+    for dirpath, dirs, names in os.walk(REF):
+        dirs[:] = [d for d in dirs if d not in (".git", "target")]
+        for n in names:
+            if n.endswith((".wgsl", ".rs")):
+                full = os.path.join(dirpath, n)
+                files[os.path.relpath(full, REF)] = full
+    return files
+
+
+def _resolve(cited, files):
+    """The reference files whose path ends with the cited path."""
+    return [f for rel, f in files.items() if rel == cited or rel.endswith("/" + cited)]
+
+
+def _repo_sources():
+    for dirpath, dirs, names in os.walk(ROOT):
+        dirs[:] = [d for d in dirs if d not in (".git", "_work", "gpurun_out", "_build", "baseline", "__pycache__")]
+        for n in names:
+            if n in SKIP_FILES or not n.endswith((".py", ".cu", ".cuh", ".h", ".cpp", ".md", "Makefile")):
+                continue
+            yield os.path.join(dirpath, n)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "RustGS")), reason="reference checkout not present")
+def test_reference_line_citations_are_in_range():
+    files = _reference_files()
+    lines = {}
+    bad, checked = [], 0
+    for path in _repo_sources():
+        for ln, text in enumerate(open(path, errors="ignore"), 1):
+            for m in CITE.finditer(text):
+                cands = _resolve(m.group(1), files)
+                # Shader names are unique; a Rust citation is checked when its
+                # path names exactly one file.
+                if len(cands) != 1:
+                    if m.group(1).endswith(".wgsl"):
+                        bad.append((os.path.relpath(path, ROOT), ln, m.group(0), "no such shader"))
+                    continue
+                f = cands[0]
+                if f not in lines:
+                    lines[f] = sum(1 for _ in open(f, errors="ignore"))
+                for part in re.split(r",\s?", m.group(2)):
+                    nums = [int(x) for x in part.split("-")]
+                    checked += 1
+                    if max(nums) > lines[f] or min(nums) < 1 or nums != sorted(nums):
+                        bad.append((os.path.relpath(path, ROOT), ln, m.group(0), f"file has {lines[f]} lines"))
+    assert checked > 100
+    assert not bad, "\n".join(map(str, bad))

@@ -1,0 +1,178 @@
+"""Parity at the sizes the numbers are quoted on.
+
+* Config 2 (200,000 Gaussians, SH degree 3, 640x480): GPU backward against
+  the oracle in both adjoint modes, and against FP64 central differences
+  (step 1e-4) on 256 seeded parameters.
+* Config 3 (1,000,000 Gaussians, SH degree 3, 8 views of 1280x720 in one
+  launch, the benchmark's workload): every view's forward bit-exact in its
+  integer outputs and within 1e-5 in its image against the FP32 oracle, with
+  the raster batches the autotuner chooses between (128, 256); the loss
+  kernel on view 0; and the gradients of view 0 for the oracle's loss
+  gradient as upstream (the other views' upstream zero) against the FP32
+  and FP64 oracles.
+"""
+import numpy as np
+import pytest
+
+from _parity import assert_forward_parity, assert_grad_close, assert_grad_parity, oracle_forward, report, \
+    run_gpu_forward
+from rustscan_b200 import scenes as S
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def _fit(ctx, splats, cams):
+    from rustscan_b200 import GsrError
+
+    for _ in range(4):
+        try:
+            ctx.render_forward(splats, cams, check=True)
+            return
+        except GsrError as e:
+            if e.status != 3:
+                raise
+            ctx.reserve_isects(int(e.required * 1.15) + 1024)
+    raise RuntimeError("could not fit intersection capacity")
+
+
+def _grads_np(g):
+    return {k: (t.cpu().numpy() if t is not None else None) for k, t in g.items()}
+
+
+@pytest.fixture(scope="module")
+def config2():
+    return S.config2()
+
+
+@pytest.mark.parametrize("mode", ["exact", "reference"])
+def test_config2_backward_full_size(gsr_ctx_factory, config2, mode):
+    import torch
+
+    from rustscan_b200 import host_splats_to_device
+
+    sc = config2
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width)
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=640 * 480, max_isects=8 << 20, adjoint=mode)
+    splats = host_splats_to_device(sc)
+    _, g = run_gpu_forward(ctx, splats, sc.cameras)
+    o = oracle_forward(sc, cam)
+    assert_forward_parity(g[0], o)
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=True))
+    torch.cuda.synchronize()
+    m = 0 if mode == "exact" else 1
+    ob = o.backward(up, mode=m)
+    od = oracle_forward(sc, cam, f64=True).backward(up, mode=m)
+    assert_grad_close(ctx.export(0, "splat_grads").reshape(-1, 12), ob["splat_grads"], rtol=1e-3,
+                      what="screen-space sums")
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"config2 {mode} {k}")
+    assert_grad_parity(gg["stats"][0], ob["stats"], od["stats"], what=f"config2 {mode} stats")
+
+
+def test_config2_gpu_gradient_vs_central_differences(gsr_ctx_factory, config2):
+    """The GPU's exact adjoint at 256 seeded parameters against FP64 central
+    differences (step 1e-4) of the oracle's render, with the FP32 oracle's
+    own gradient as the yardstick (assert_grad_parity with the differences in
+    the FP64 role). Parameters whose step flips a blend decision are set
+    aside (tests/_fd.py)."""
+    import torch
+
+    from _fd import analytic, local_central_differences, sample_params
+    from oracle import oracle as O
+    from rustscan_b200 import host_splats_to_device
+
+    sc = config2
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width)
+    base64 = O.Forward(sc.transforms.astype(np.float64), sc.sh.astype(np.float64),
+                       sc.raw_opacity.astype(np.float64), 3, cam, f64=True)
+    params = sample_params(base64, 256, seed=2)
+    fd, flips, _ = local_central_differences(sc, cam, up.astype(np.float64), params, h=1e-4)
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=640 * 480, max_isects=8 << 20)
+    splats = host_splats_to_device(sc)
+    ctx.render_forward(splats, sc.cameras)
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=False))
+    r32 = oracle_forward(sc, cam).backward(up, mode=0)
+    smooth = ~flips
+    g_s = np.array([analytic(gg, p) for p in params])[smooth]
+    r_s = np.array([analytic(r32, p) for p in params])[smooth]
+    assert flips.sum() <= 0.15 * len(params)
+    assert_grad_parity(g_s, r_s, fd[smooth], rtol=1e-4, what="config2 gpu vs fp64 central differences")
+
+
+# ---- config 3: the benchmark workload ---------------------------------------------
+
+
+@pytest.fixture(scope="module")
+def config3():
+    from oracle import oracle as O
+
+    sc = S.config3()
+    gt = S.config3_targets()
+    cam = sc.cameras[0]
+    target = O.Forward(gt[0], gt[1], gt[2], 3, cam).image[..., :3].copy()
+    return sc, target
+
+
+@pytest.mark.parametrize("batch", [128, 256])
+def test_config3_forward_all_views(gsr_ctx_factory, config3, batch):
+    """All 8 views of one batched launch against the FP32 oracle, view by view."""
+    import torch
+
+    from rustscan_b200 import host_splats_to_device
+
+    sc, _ = config3
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=8, max_pixels=1280 * 720, max_isects=24 << 20, batch=batch)
+    splats = host_splats_to_device(sc)
+    _fit(ctx, splats, sc.cameras)
+    _, g = run_gpu_forward(ctx, splats, sc.cameras)
+    torch.cuda.synchronize()
+    views = range(8) if batch == 128 else (0, 5)
+    for v in views:
+        o = oracle_forward(sc, sc.cameras[v])
+        assert o.num_intersections > 1_000_000
+        assert_forward_parity(g[v], o)
+        report(f"config3 view {v} forward (batch {batch})", visible=o.num_visible, intersections=o.num_intersections,
+               image_max_abs=float(np.abs(g[v]["image"] - o.image).max()))
+        del o
+
+
+def test_config3_view0_loss_and_gradients(gsr_ctx_factory, config3):
+    import torch
+
+    from oracle import oracle as O
+    from rustscan_b200 import host_splats_to_device
+
+    sc, target = config3
+    cams = sc.cameras
+    cam = cams[0]
+    H, W = cam.height, cam.width
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=8, max_pixels=1280 * 720, max_isects=24 << 20, batch=128)
+    splats = host_splats_to_device(sc)
+    _fit(ctx, splats, cams)
+    o = oracle_forward(sc, cam)
+    val, vp = O.loss(o.image, target)
+
+    # The loss kernel on the oracle's image of view 0.
+    loss, vpg = ctx.loss(torch.as_tensor(np.ascontiguousarray(o.image, np.float32), device="cuda"),
+                         torch.as_tensor(target, device="cuda"), [cam])
+    torch.cuda.synchronize()
+    assert abs(float(loss[0]) - val) <= 1e-5 * abs(val), (float(loss[0]), val)
+    vpg = vpg.cpu().numpy()
+    np.testing.assert_allclose(vpg, vp, rtol=1e-4, atol=1e-4 * float(np.abs(vp).max()))
+
+    # Gradients of view 0 inside the 8-view launch.
+    ctx.render_forward(splats, cams)
+    up = np.zeros((8, H, W, 4), np.float32)
+    up[0] = vp
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up.reshape(-1), device="cuda"), stats=True))
+    torch.cuda.synchronize()
+    ob = o.backward(vp, mode=0)
+    od = oracle_forward(sc, cam, f64=True).backward(vp.astype(np.float64), mode=0)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"config3 view 0 {k}")
+    assert_grad_parity(gg["stats"][0], ob["stats"], od["stats"], what="config3 view 0 stats")
+    # The other views' gradient columns (signed and absolute mean-gradient
+    # sums) are zero under a zero upstream gradient.
+    assert not gg["stats"][1:, :, 0:5].any()

@@ -177,6 +177,48 @@ def test_exact_adjoint_matches_fp64_finite_differences():
     assert np.median(errs) < 1e-6 and np.quantile(errs, 0.9) < 1e-4, errs
 
 
+def test_config2_adjoint_matches_fp64_central_differences():
+    """The adjoint check at config 2's full size (200,000 Gaussians, SH degree
+    3, 640x480): FP64 central differences with step 1e-4 on 256 seeded
+    parameters of contributing Gaussians (a third each transforms columns, SH
+    coefficients, opacity logits) against the FP64 exact adjoint, and the
+    reference-semantics gradient (project_backwards.wgsl without the
+    compensation and view-direction terms, rasterize_backwards.wgsl's
+    termination) measured against the same differences. Differences are
+    taken over the tiles the perturbed Gaussian touches (tests/_fd.py); a
+    parameter whose step flips a blend decision of some pixel is set aside
+    (the adjoint of a discontinuity is not defined) and counted."""
+    from _fd import analytic, local_central_differences, sample_params
+    from _parity import report
+
+    sc = S.config2()
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width).astype(np.float64)
+    base = O.Forward(sc.transforms.astype(np.float64), sc.sh.astype(np.float64), sc.raw_opacity.astype(np.float64),
+                     3, cam, f64=True)
+    params = sample_params(base, 256, seed=2)
+    fd, flips, base = local_central_differences(sc, cam, up, params, h=1e-4)
+    exact = base.backward(up, mode=0)
+    refg = base.backward(up, mode=1)
+    an = np.array([analytic(exact, p) for p in params])
+    ar = np.array([analytic(refg, p) for p in params])
+    den = lambda a: np.maximum(np.maximum(np.abs(fd), np.abs(a)), 1e-6)  # noqa: E731
+    e_exact = np.abs(fd - an) / den(an)
+    e_ref = np.abs(fd - ar) / den(ar)
+    smooth = ~flips
+    report("config2 fd (fp64 exact adjoint)", n=len(params), flipped=int(flips.sum()),
+           median=float(np.median(e_exact[smooth])), p90=float(np.quantile(e_exact[smooth], 0.9)),
+           max=float(e_exact[smooth].max()))
+    report("config2 fd (reference-semantics gradient)", n=len(params), flipped=int(flips.sum()),
+           median=float(np.median(e_ref[smooth])), p90=float(np.quantile(e_ref[smooth], 0.9)),
+           max=float(e_ref[smooth].max()))
+    assert flips.sum() <= 0.15 * len(params), int(flips.sum())
+    assert np.median(e_exact[smooth]) < 1e-6, np.median(e_exact[smooth])
+    assert e_exact[smooth].max() < 1e-4, (e_exact[smooth].max(), params[int(np.argmax(np.where(smooth, e_exact, 0)))])
+    # The reference semantics drop two terms of the true derivative.
+    assert np.median(e_ref[smooth]) > 100 * np.median(e_exact[smooth])
+
+
 def test_reference_mode_equals_literal_wgsl_walk():
     sc = S.small_scene(n=1500, degree=2, width=64, height=48, seed=8)
     cam = sc.cameras[0]
@@ -373,7 +415,7 @@ def _fma(a, b, c):
 
 def test_forward_blend_matches_independent_restatement():
     """The FP64 oracle's front-to-back blend against a restatement of
-    rasterize.wgsl:257-276 per pixel: sigma in the WGSL operation order,
+    rasterize.wgsl:54-88 per pixel: sigma in the WGSL operation order,
     alpha = min(0.999, opacity * exp(-sigma)) taken when sigma >= 0 and
     alpha >= 1/255, colour += max(c, 0) * alpha * T as one fused multiply-add,
     T *= 1 - alpha, stop once T < 1e-4. Every output is compared bit for bit."""
@@ -509,7 +551,7 @@ def _standard_sh_color(degree, d, sh):
 
 @pytest.mark.parametrize("degree", [1, 2, 3])
 def test_sh_colour_matches_standard_real_sh(degree):
-    """project_visible.wgsl:141-224 evaluates the basis in a factored form;
+    """project_visible.wgsl:44-127 evaluates the basis in a factored form;
     the oracle's colours (FP64) against the textbook terms."""
     sc = S.small_scene(n=300, degree=degree, width=80, height=60, seed=4, logscale_mu=-2.5)
     cam = sc.cameras[0]
