@@ -27,6 +27,9 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd ms/view (1M Gaussians, 1280x720) batched vs plain; grad rel err"
 UNIT = "ms/view"
 WORKLOAD = "batched training step: 1,000,000 Gaussians, SH degree 3, 8 views of 1280x720 per step"
+# ncu smsp__inst_executed.sum of the raster kernels on one 1280x720 view of
+# this workload (6,273,269 intersections), per intersection.
+WARP_INST_PER_ISECT = {"raster_bwd": 205.9e6 / 6273269, "raster_fwd": 152.5e6 / 6273269}
 
 
 def parse():
@@ -41,6 +44,9 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-bf16", action="store_true", help="skip the BF16-storage batched timing")
     p.add_argument("--no-precision", action="store_true", help="skip the FP64 precision report (CPU baseline leg)")
+    p.add_argument("--config", default="c3", choices=["c1", "c3", "c4", "c5"],
+                   help="c3 (default): the batched training step the metric is quoted on; c1, c4, c5: the other "
+                        "configurations' workloads, one JSON line each")
     p.add_argument("--mode", default="bench", choices=["bench", "profile"],
                    help="profile: warm up, then run exactly one non-graph batched step (for ncu launch lists)")
     return p.parse_args()
@@ -342,8 +348,244 @@ def profile_step(args):
     print(json.dumps({"profile_step": "done", "views": len(cams), "n": args.n}), flush=True)
 
 
+def _time_device(fn, steps, warmup):
+    """Mean device ms of fn() over `steps` calls after `warmup`, CUDA events on the current stream."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _render_op_line(args, name, sc, contexts, workload, dtype, extra=None):
+    """fwd+bwd ms/view of the render op (gsr_render_forward + gsr_render_backward,
+    one view per call, an N(0,1) upstream image gradient) for each named context
+    configuration; the first is the headline of the line. End to end: the
+    upstream gradient crosses from pinned host memory and the image comes back
+    each step."""
+    import torch
+
+    from rustscan_b200 import Context, host_splats_to_device
+    from rustscan_b200 import scenes as S
+
+    cam = sc.cameras[0]
+    H, W = cam.height, cam.width
+    up = torch.as_tensor(S.upstream_grad(H, W), device="cuda")
+    res = {}
+    first = None
+    for label, kw in contexts:
+        ctx = Context(max_splats=sc.n, max_pixels=W * H, max_isects=kw.pop("max_isects", 16 << 20), **kw)
+        splats = host_splats_to_device(sc, sh_dtype=torch.bfloat16 if kw.get("sh_dtype") == "bf16" else torch.float32)
+        fit_capacity(ctx, splats, [cam])
+
+        def step():
+            ctx.render_forward(splats, [cam], check=False)
+            ctx.render_backward(splats, up, stats=True)
+
+        ms = _time_device(step, args.steps, args.warmup)
+        res[label] = {"ms_per_view": ms}
+        if first is None:
+            first = (label, ctx, splats, ms)
+        else:
+            ctx.close()
+    label, ctx, splats, ms = first
+    up_h = torch.empty_like(up, device="cpu").pin_memory()
+    up_h.copy_(up.cpu())
+    img_h = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    up_d = torch.empty_like(up)
+
+    def e2e_step():
+        up_d.copy_(up_h, non_blocking=True)
+        _, imgs, _ = ctx.render_forward(splats, [cam], check=False)
+        ctx.render_backward(splats, up_d, stats=True)
+        img_h.copy_(imgs[0], non_blocking=True)
+
+    ms_e2e = _time_device(e2e_step, args.steps, args.warmup)
+    counts = ctx.export(0, "counts")
+    evals = int(ctx.export(0, "nvisit").astype(np.int64).sum())
+    ctx.close()
+    line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded; see rustscan_b200/scenes.py)",
+            "config": {"workload": workload, "n_gaussians": sc.n, "resolution": f"{W}x{H}", "sh_degree": sc.sh_degree,
+                       "visible": int(counts[0]), "intersections": int(counts[1]), "headline": label},
+            "paths_ms_per_view": res, "gaussian_pixel_evals_per_view": evals,
+            "gaussian_pixel_evals_per_s": evals / (ms * 1e-3),
+            "e2e": {"value": ms_e2e, "unit": UNIT, "h2d_bytes_per_step": int(up.numel() * 4),
+                    "d2h_bytes_per_step": int(H * W * 16),
+                    "inputs": "upstream image gradient from pinned host memory; rendered image read back"},
+            "gpu_launches": None}
+    if extra:
+        line.update(extra)
+    return line
+
+
+def bench_config1(args):
+    """Config 1: plain FP32 forward + backward of one 256x256 view (16,384
+    Gaussians, SH degree 0), beside the CPU path on the same view."""
+    from oracle import oracle as O
+    from rustscan_b200 import scenes as S
+
+    sc = S.config1()
+    line = _render_op_line(args, "c1", sc, [("f32", {})],
+                           "plain FP32 forward+backward, single view: 16,384 Gaussians, SH degree 0, 256x256", "f32")
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 0, cam).backward(up, mode=0)
+    cpu_ms = (time.perf_counter() - t0) * 1000.0 / reps
+    t1 = time.perf_counter()
+    for _ in range(reps):
+        O.ref_cpu_forward(sc, cam)
+    ref_ms = (time.perf_counter() - t1) * 1000.0 / reps
+    line["cpu_baseline"] = {"value": cpu_ms, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                            "sample": f"the same view, {reps} repetitions: oracle forward + exact backward, OpenMP over "
+                                      "all host threads",
+                            "reference_cpu_forward": {"value": ref_ms, "unit": UNIT, "cores": 1,
+                                                      "sample": "the reference's shipped CPU renderer (forward only)"}}
+    return line
+
+
+def bench_config4(args):
+    """Config 4: 3M Gaussians (5% flattened), one 1920x1080 view, fx = 1400:
+    forward + backward with BF16 SH storage and the FP64 conic (the headline)
+    beside plain FP32; precision of both against the FP64 oracle."""
+    import torch
+
+    from oracle import oracle as O
+    from rustscan_b200 import Context, host_splats_to_device
+    from rustscan_b200 import scenes as S
+
+    sc = S.config4()
+    line = _render_op_line(args, "c4", sc, [("bf16_sh_fp64_conic", {"sh_dtype": "bf16", "fp64_conic": True,
+                                                                     "max_isects": 48 << 20}),
+                                            ("f32", {"max_isects": 48 << 20})],
+                           "mixed-precision render+backward: 3,000,000 Gaussians (5% flattened), SH degree 3, "
+                           "1920x1080", "bf16 storage, f32 blend")
+    if args.no_precision:
+        return line
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width)
+    sh_bf = torch.as_tensor(sc.sh).to(torch.bfloat16).float().numpy()
+    prec = {}
+    t0 = time.perf_counter()
+    u64 = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, 3, cam, f64=True)
+    g_u64 = u64.backward(up.astype(np.float64), mode=0)
+    oracle_s = time.perf_counter() - t0
+    for name, kw, sh_ref in (("f32", {}, None), ("bf16_sh_fp64_conic", {"sh_dtype": "bf16", "fp64_conic": True}, sh_bf)):
+        ctx = Context(max_splats=sc.n, max_pixels=cam.width * cam.height, max_isects=48 << 20, **kw)
+        sp = host_splats_to_device(sc, sh_dtype=torch.bfloat16 if kw.get("sh_dtype") == "bf16" else torch.float32)
+        fit_capacity(ctx, sp, [cam])
+        _, imgs, _ = ctx.render_forward(sp, [cam])
+        g = ctx.render_backward(sp, torch.as_tensor(up, device="cuda"), stats=False)
+        torch.cuda.synchronize()
+        img = imgs[0].cpu().numpy()
+        gg = {k: g[k].cpu().numpy() for k in ("v_transforms", "v_sh", "v_raw_opacity")}
+        ctx.close()
+        e = {"image_psnr_vs_fp64_db": _psnr(img[..., :3], u64.image[..., :3]),
+             "image_max_abs_vs_fp64": float(np.abs(img - u64.image).max()),
+             "grad_rel_err_vs_fp64": _grad_rel(gg, g_u64)}
+        if sh_ref is not None:
+            r64 = O.Forward(sc.transforms, sh_ref, sc.raw_opacity, 3, cam, f64=True)
+            e["image_psnr_vs_fp64_of_stored_params_db"] = _psnr(img[..., :3], r64.image[..., :3])
+            e["grad_rel_err_vs_fp64_of_stored_params"] = _grad_rel(gg, r64.backward(up.astype(np.float64), mode=0))
+            del r64
+        prec[name] = e
+    prec["against"] = ("the FP64 oracle of the scene as given (unrounded parameters); for BF16 also the FP64 oracle "
+                       "of the stored, BF16-rounded SH")
+    prec["oracle_fp64_seconds"] = oracle_s
+    line["precision"] = prec
+    return line
+
+
+def bench_config5(args):
+    """Config 5: 32 views of mixed resolution over 2M Gaussians (BF16 SH
+    storage), tile shape and raster batch from the autotuner: the batched
+    training step (one launch per stage over all views, graph-replayed)
+    against the plain single-view path (one view per call, no graph), per
+    view; plus the batched step in FP32."""
+    import torch
+
+    from rustscan_b200 import Context, LearningRates, Trainer, autotune, host_splats_to_device
+    from rustscan_b200 import scenes as S
+
+    sc = S.config5()
+    cams = sc.cameras
+    nv = len(cams)
+    pmax = max(c.width * c.height for c in cams)
+    splats = host_splats_to_device(sc, sh_dtype=torch.bfloat16)
+    tuned = autotune(splats, cams, reps=1, max_pixels=pmax, max_isects=24 << 20, sh_dtype="bf16")
+    tile, batch = tuned["tile"], tuned["batch"]
+    rng = np.random.default_rng(5)
+    targets = torch.as_tensor(np.concatenate([rng.uniform(0, 1, c.width * c.height * 3) for c in cams])
+                              .astype(np.float32), device="cuda")
+    offs = np.concatenate([[0], np.cumsum([c.width * c.height * 3 for c in cams])])
+
+    def batched_ms(sh_dtype, sp):
+        ctx = Context(max_splats=sc.n, max_views=nv, max_pixels=pmax, max_isects=24 << 20, sh_dtype=sh_dtype,
+                      tile=tile, batch=batch)
+        fit_capacity(ctx, sp, cams)
+        counts = [ctx.export(v, "counts") for v in range(nv)]
+        tr = Trainer(ctx, sp, LearningRates(), total_iterations=30000, use_graph=True)
+        ms = time_steps(lambda it: tr.train_step(cams, targets, it), args.steps, args.warmup, 1)
+        stages = stage_profile(ctx, lambda: Trainer(ctx, sp, LearningRates(), use_graph=False).train_step(
+            cams, targets, args.warmup + args.steps + 1))
+        ctx.close()
+        return ms / args.steps / nv, counts, stages
+
+    ms_b, counts, stages = batched_ms("bf16", splats)
+    # Plain path: one view per call, in a context sized for one view.
+    ctx1 = Context(max_splats=sc.n, max_views=1, max_pixels=pmax, max_isects=24 << 20, sh_dtype="bf16", tile=tile,
+                   batch=batch)
+    fit_capacity(ctx1, splats, [max(cams, key=lambda c: c.width * c.height)])
+    tr1 = Trainer(ctx1, splats, LearningRates(), use_graph=False)
+    per_view = []
+    for v, cam in enumerate(cams):
+        fit_capacity(ctx1, splats, [cam])
+        tv = targets[offs[v]:offs[v + 1]]
+        per_view.append(time_steps(lambda it: tr1.train_step([cam], tv, it), max(2, args.steps // 2), 1, 1)
+                        / max(2, args.steps // 2))
+    ctx1.close()
+    splats32 = host_splats_to_device(sc)
+    ms_f32, _, _ = batched_ms("f32", splats32)
+    V = [int(c[0]) for c in counts]
+    I = [int(c[1]) for c in counts]
+    plain = float(np.mean(per_view))
+    return {"metric": METRIC, "value": ms_b, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b * nv, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 storage, f32 blend", "data": "synthetic (seeded; see rustscan_b200/scenes.py)",
+            "config": {"workload": "uneven batch: 32 views of mixed resolution (320x240 to 1920x1080), 2,000,000 "
+                                   "Gaussians, SH degree 3, BF16 SH storage, one training step over all views",
+                       "resolutions": [f"{c.width}x{c.height}" for c in cams], "visible_per_view": V,
+                       "intersections_per_view": I, "tile": f"{tile[0]}x{tile[1]}", "raster_batch": batch,
+                       "tile_and_batch": "autotuner (gsr_autotune)", "graph": True},
+            "plain_single_view_ms_per_view": plain, "plain_per_view_ms": per_view,
+            "batched_over_plain": ms_b / plain, "f32_batched_ms_per_view": ms_f32,
+            "stages_ms_per_step": stages, "gpu_launches": None}
+
+
 def main():
     args = parse()
+    if args.config != "c3":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm is timed on the c3 workload"}))
+            return
+        import torch
+
+        torch.cuda.set_device(0)
+        fn = {"c1": bench_config1, "c4": bench_config4, "c5": bench_config5}[args.config]
+        print(json.dumps(fn(args)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -436,7 +678,26 @@ def main():
         traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                "algorithmic_bytes": algo[dom], "launch_ms": stages[dom]}
+                "algorithmic_bytes": algo[dom], "launch_ms": stages[dom],
+                "traffic_over_algorithmic": (traffic / algo[dom]) if traffic else None}
+    # The raster kernels are bound by instruction issue, not by HBM: their
+    # issue roofline is the SMs' warp-instruction issue rate (4 schedulers
+    # per SM, one warp instruction each per clock) at the SM clock measured
+    # during the timed region. The warp instructions per launch come from
+    # one ncu capture of a single 1280x720 view (smsp__inst_executed.sum),
+    # scaled to the launch by its intersections.
+    inst_per_isect = {"raster_bwd": WARP_INST_PER_ISECT["raster_bwd"], "raster_fwd": WARP_INST_PER_ISECT["raster_fwd"]}
+    sm_mhz = clk.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    if dom in inst_per_isect:
+        winst = inst_per_isect[dom] * sum(I)
+        peak_issue = n_sm * 4 * sm_mhz * 1e6
+        roofline["issue"] = {"bound": "issue", "achieved": winst / (stages[dom] * 1e-3) / 1e9,
+                             "peak": peak_issue / 1e9, "unit": "G warp-instructions/s",
+                             "frac": winst / (stages[dom] * 1e-3) / peak_issue, "warp_instructions": winst,
+                             "sm_mhz": sm_mhz, "sms": n_sm,
+                             "source": "warp instructions per intersection from ncu smsp__inst_executed.sum on one "
+                                       "view, times this launch's intersections"}
 
     # ---- the same batched step with BF16 SH storage ---------------------------
     bf16_ms = None
