@@ -97,10 +97,15 @@ def host_splats_to_device(scene, device="cuda", sh_dtype=torch.float32) -> Devic
     )
 
 
+SCHEDULES = {"default": _lib.GSR_SCHEDULE_DEFAULT, "persistent": _lib.GSR_SCHEDULE_PERSISTENT,
+             "grid": _lib.GSR_SCHEDULE_GRID}
+
+
 def make_config(max_splats, max_views=1, max_pixels=1920 * 1080, max_isects=0, tile=(16, 16), sh_dtype="f32",
                 adjoint="exact", deterministic=False, fp64_conic=False, cov_blur=DEFAULT_RASTER_COV_BLUR,
-                background=(0.0, 0.0, 0.0), batch=0) -> _lib.gsr_config:
-    """The gsr_config of a context (include/gsr.h)."""
+                background=(0.0, 0.0, 0.0), batch=0, schedule="default") -> _lib.gsr_config:
+    """The gsr_config of a context (include/gsr.h). schedule: "default",
+    "persistent" (cost-ordered work queue) or "grid" (one CTA per tile)."""
     cfg = _lib.gsr_config()
     cfg.cov_blur = float(cov_blur)
     for i in range(3):
@@ -115,6 +120,7 @@ def make_config(max_splats, max_views=1, max_pixels=1920 * 1080, max_isects=0, t
     cfg.max_views = int(max_views)
     cfg.max_pixels = int(max_pixels)
     cfg.max_isects = int(max_isects)
+    cfg.schedule = SCHEDULES[schedule]
     return cfg
 
 
@@ -145,11 +151,11 @@ class Context:
 
     def __init__(self, max_splats, max_views=1, max_pixels=1920 * 1080, max_isects=0, tile=(16, 16),
                  sh_dtype="f32", adjoint="exact", deterministic=False, fp64_conic=False,
-                 cov_blur=DEFAULT_RASTER_COV_BLUR, background=(0.0, 0.0, 0.0), batch=0):
+                 cov_blur=DEFAULT_RASTER_COV_BLUR, background=(0.0, 0.0, 0.0), batch=0, schedule="default"):
         _require_cuda()
         self._lib = _lib.load()
         cfg = make_config(max_splats, max_views, max_pixels, max_isects, tile, sh_dtype, adjoint, deterministic,
-                          fp64_conic, cov_blur, background, batch)
+                          fp64_conic, cov_blur, background, batch, schedule)
         self.cfg = cfg
         self.background = tuple(float(b) for b in background)
         h = C.c_void_p()

@@ -28,6 +28,9 @@ GSR_SH_F32 = 0
 GSR_SH_BF16 = 1
 GSR_ADJOINT_EXACT = 0
 GSR_ADJOINT_REFERENCE = 1
+GSR_SCHEDULE_DEFAULT = 0
+GSR_SCHEDULE_PERSISTENT = 1
+GSR_SCHEDULE_GRID = 2
 
 
 class gsr_config(C.Structure):
@@ -43,7 +46,7 @@ class gsr_config(C.Structure):
         ("fp64_conic", C.c_int32),
         ("max_splats", C.c_uint64),
         ("max_views", C.c_uint32),
-        ("_pad0", C.c_uint32),
+        ("schedule", C.c_uint32),
         ("max_pixels", C.c_uint64),
         ("max_isects", C.c_uint64),
     ]

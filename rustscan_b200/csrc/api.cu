@@ -154,7 +154,8 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.ranges, nv * 2 * T) && dalloc(c, &b.tfinal, nv * P) && dalloc(c, &b.last, nv * P) &&
             dalloc(c, &b.ncontrib, nv * P) && dalloc(c, &b.nvisit, nv * P) && dalloc(c, &b.visible_c, nv * V) &&
             dalloc(c, &b.sgrad, nv * V * 3) && dalloc(c, &b.pair, nv * V * 6) && dalloc(c, &b.vcount, nv * 4) &&
-            dalloc(c, &b.tile_hist, nv * T) && dalloc(c, &b.hitw, nv * I);
+            dalloc(c, &b.tile_hist, nv * T) && dalloc(c, &b.hitw, nv * I) && dalloc(c, &b.sched_order, nv * T) &&
+            dalloc(c, &b.sched_work, nv * T) && dalloc(c, &b.sched_ticket, 1);
   b.proj_parts_cap = (uint32_t)((N + 255) / 256);
   ok = ok && dalloc(c, &b.vis_bits, nv * b.proj_parts_cap * 8) && dalloc(c, &b.blk_count, nv * b.proj_parts_cap) &&
        dalloc(c, &b.blk_base, nv * b.proj_parts_cap);
@@ -241,6 +242,7 @@ gsr_status build_views(gsr_ctx* c, const gsr_camera* cams, uint32_t n_views, std
   vs.batch = c->cfg.batch;
   vs.total_tiles = tile_base;
   vs.max_tiles = max_tiles;
+  vs.persistent = c->cfg.schedule == GSR_SCHEDULE_PERSISTENT;
   return GSR_OK;
 }
 
@@ -366,6 +368,7 @@ gsr_status gsr_create(const gsr_config* cfg_in, gsr_ctx** out) {
     cfg.tile_h = 16;
   }
   if (cfg.max_views == 0) cfg.max_views = 1;
+  if (cfg.schedule == GSR_SCHEDULE_DEFAULT) cfg.schedule = GSR_SCHEDULE_PERSISTENT;
   if (cfg.max_splats == 0) cfg.max_splats = 1u << 16;
   if (cfg.max_pixels == 0) cfg.max_pixels = 1920ull * 1080ull;
   if (cfg.max_isects == 0) cfg.max_isects = std::min<uint64_t>(std::max<uint64_t>(16 * cfg.max_splats, 1u << 20), 1ull << 29);
@@ -379,6 +382,8 @@ gsr_status gsr_create(const gsr_config* cfg_in, gsr_ctx** out) {
     st = fail(c, GSR_ERR_INVALID_ARG, "unknown sh_dtype");
   else if (!(cfg.cov_blur >= 0.f))
     st = fail(c, GSR_ERR_INVALID_ARG, "cov_blur must be >= 0");
+  else if (cfg.schedule != GSR_SCHEDULE_PERSISTENT && cfg.schedule != GSR_SCHEDULE_GRID)
+    st = fail(c, GSR_ERR_INVALID_ARG, "unknown schedule");
   if (st != GSR_OK) {
     gsr_status r = st;
     delete c;

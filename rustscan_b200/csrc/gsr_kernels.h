@@ -44,6 +44,9 @@ struct FwdBufs {
   float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)
   uint32_t* inv_perm;      // [I] emission index -> sorted position (deterministic mode)
   uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
+  uint32_t* sched_order;   // [views * Tcap] raster work items in issue order (persistent schedule)
+  uint32_t* sched_work;    // [views * Tcap] per work item: list entries up to the tile's last contributor
+  uint32_t* sched_ticket;  // [1] next slot of sched_order a persistent raster CTA takes
   uint64_t Vcap, Ncap, Icap, Tcap, Pcap;
   uint32_t pack_bits;      // > 0: intersections are packed keys (see isect_key), else (tile, index) pairs
   bool slots;              // slot layout: one key per box tile, sentinel keys last; vcount[3] = keys sorted
@@ -64,6 +67,7 @@ struct ViewSet {
   uint32_t batch;         // Gaussians per shared-memory batch of the rasterizer (0: tuned defaults)
   uint32_t total_tiles;   // sum over views of tiles_x * tiles_y
   uint32_t max_tiles;     // max over views
+  int persistent;         // raster work: 1 persistent CTAs taking cost-ordered items, 0 one CTA per item
 };
 
 struct SplatsDev {

@@ -28,6 +28,19 @@
 // memory in warp order, and over tiles from float4 atomics (or, in
 // deterministic mode, per-intersection records reduced later in a fixed
 // order).
+//
+// Work items are the (view, tile) pairs of the launch. With the persistent
+// schedule a single-block kernel first orders the items by decreasing
+// estimated cost (counting sort over the bit length of the cost: the list
+// length for the forward, the entries up to the tile's last contributor for
+// the backward, which the forward records per item), and the raster kernels
+// run as many CTAs as the SMs hold at once, each taking the next item from
+// an atomic ticket. The longest tiles start first, so the launch does not
+// end in a tail of long tiles on a few SMs; views of different sizes and
+// visible counts share one queue. Otherwise one CTA per item runs in item
+// order.
+#include <algorithm>
+
 #include "gsr_kernels.h"
 
 namespace gsr {
@@ -56,6 +69,59 @@ __device__ __forceinline__ uint32_t find_view(const ViewSet& vs, uint32_t item) 
   for (uint32_t i = 1; i < vs.n_views; ++i)
     if (vs.views[i].tile_base <= item) v = i;
   return v;
+}
+
+constexpr uint32_t kNoItem = 0xffffffffu;
+
+// The next work item of this CTA (block-uniform; kNoItem when done). In
+// the grid schedule a CTA runs item blockIdx.x once; in the persistent one
+// thread 0 takes a ticket and reads the item at that slot of the cost order.
+// The leading barrier keeps the previous item's shared state intact until
+// every thread is done with it.
+__device__ __forceinline__ uint32_t next_item(const RasterArgs& a, uint32_t round, uint32_t* s_item) {
+  if (!a.vs.persistent) return round == 0 ? blockIdx.x : kNoItem;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t slot = atomicAdd(a.b.sched_ticket, 1u);
+    *s_item = slot < a.vs.total_tiles ? a.b.sched_order[slot] : kNoItem;
+  }
+  __syncthreads();
+  return *s_item;
+}
+
+__device__ __forceinline__ uint32_t cost_bucket(uint32_t cost) { return cost ? 32u - (uint32_t)__clz(cost) : 0u; }
+
+// One block: the work items of the launch in decreasing order of cost
+// bucket (bit length of the cost; order within a bucket is arbitrary), and
+// the ticket reset. BWD selects the backward's cost (recorded by the
+// forward), else the list length.
+constexpr int kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads) sched_order_kernel(ViewSet vs, FwdBufs b, int bwd) {
+  __shared__ uint32_t s_hist[33];
+  __shared__ uint32_t s_start[33];
+  if (threadIdx.x < 33) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t total = vs.total_tiles;
+  auto cost_of = [&](uint32_t item) -> uint32_t {
+    if (bwd) return b.sched_work[item];
+    const uint32_t v = find_view(vs, item);
+    const uint32_t t = item - vs.views[v].tile_base;
+    const uint32_t* r = slice(b.ranges, 2 * b.Tcap, v);
+    return r[2 * t + 1] - r[2 * t];
+  };
+  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads) atomicAdd(&s_hist[cost_bucket(cost_of(i))], 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 32; k >= 0; --k) {
+      s_start[k] = run;
+      run += s_hist[k];
+    }
+    *b.sched_ticket = 0u;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads)
+    b.sched_order[atomicAdd(&s_start[cost_bucket(cost_of(i))], 1u)] = i;
 }
 
 // Warp w of a TW-wide tile owns the 8 x (4*PPL) block at (x0, y0); lane l
@@ -185,166 +251,184 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   __shared__ uint8_t s_mask[BATCH];
   __shared__ uint8_t s_hit[NW][BATCH];  // warp w took entry j
   __shared__ uint16_t s_list[NW][BATCH];
-  const uint32_t item = blockIdx.x;
-  const uint32_t v = find_view(a.vs, item);
-  const ViewDesc& vd = a.vs.views[v];
-  const uint32_t t = item - vd.tile_base;
-  const uint32_t tx = t % vd.tiles_x, ty = t / vd.tiles_x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t px = tx * TW + WarpBlock<TW, PPL>::x0(warp) + (lane & 7);
-  const uint32_t pyb = ty * TH + WarpBlock<TW, PPL>::y0(warp) + (lane >> 3);
-  const float pcx = (float)px + 0.5f;
-  const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
-  const uint32_t s0 = ranges[2 * t], s1 = ranges[2 * t + 1];
-  const uint32_t* vals = isect_index_src(a.b, v);
-  const uint32_t vmask = isect_index_mask(a.b);
-  const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
-  uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
-  uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
-  const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
-  // Pixel q = 2k + h sits at row pyb + 4q and is half h of pair k.
-  float2 T[NP], C0[NP], C1[NP], C2[NP], npcy[NP];
-  uint32_t last[PPL], nc[PPL];  // a pixel that saturates stops at its last contributor
-  bool done[PPL];
-  bool all_done = true;
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    T[k] = f2(1.f);
-    C0[k] = C1[k] = C2[k] = f2(0.f);
-    npcy[k] = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
-  }
-#pragma unroll
-  for (int q = 0; q < PPL; ++q) {
-    const uint32_t py = pyb + 4 * q;
-    last[q] = nc[q] = 0;
-    done[q] = !(px < vd.w && py < vd.h);
-    all_done = all_done && done[q];
-  }
-  for (uint32_t b0 = s0; b0 < s1; b0 += BATCH) {
-    const uint32_t nb = min((uint32_t)BATCH, s1 - b0);
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += NT) {
-      const uint32_t c = vals[b0 + j] & vmask;
-      float4 A, B, Cc;
-      s_mask[j] = (uint8_t)stage_one<TW, PPL, NW>(rec, c, tx0, ty0, A, B, Cc);
-      s_a[j] = A;
-      s_b[j] = B;
-      s_c[j] = Cc;
-      s_cidx[j] = c;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) s_hit[w][j] = 0;
+  __shared__ uint32_t s_item;
+  __shared__ uint32_t s_work;
+  if (threadIdx.x == 0) s_work = 0u;
+  for (uint32_t round = 0;; ++round) {
+    const uint32_t item = next_item(a, round, &s_item);
+    if (item == kNoItem) break;
+    const uint32_t v = find_view(a.vs, item);
+    const ViewDesc& vd = a.vs.views[v];
+    const uint32_t t = item - vd.tile_base;
+    const uint32_t tx = t % vd.tiles_x, ty = t / vd.tiles_x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t px = tx * TW + WarpBlock<TW, PPL>::x0(warp) + (lane & 7);
+    const uint32_t pyb = ty * TH + WarpBlock<TW, PPL>::y0(warp) + (lane >> 3);
+    const float pcx = (float)px + 0.5f;
+    const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
+    const uint32_t s0 = ranges[2 * t], s1 = ranges[2 * t + 1];
+    const uint32_t* vals = isect_index_src(a.b, v);
+    const uint32_t vmask = isect_index_mask(a.b);
+    const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
+    uint8_t* vis = slice(a.b.visible_c, a.b.Vcap, v);
+    uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
+    const float tx0 = (float)(tx * TW), ty0 = (float)(ty * TH);
+    // Pixel q = 2k + h sits at row pyb + 4q and is half h of pair k.
+    float2 T[NP], C0[NP], C1[NP], C2[NP], npcy[NP];
+    uint32_t last[PPL], nc[PPL];  // a pixel that saturates stops at its last contributor
+    bool done[PPL];
+    bool all_done = true;
+  #pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      T[k] = f2(1.f);
+      C0[k] = C1[k] = C2[k] = f2(0.f);
+      npcy[k] = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
     }
-    __syncthreads();
-    if (!__all_sync(0xffffffffu, all_done)) {
-      const int cnt = build_list(s_mask, nb, 1u << warp, lane, s_list[warp]);
-      // Entries go two at a time: the sigma, cut test, exponential and
-      // contribution test of both (independent of the pixel state) form one
-      // straight-line block whose chains interleave; the blends then apply
-      // in list order, the second gated by the pixel state the first left.
-      for (int e = 0; e < cnt; e += 2) {
-        const bool two = e + 1 < cnt;  // warp-uniform
-        const uint32_t jj[2] = {s_list[warp][e], two ? s_list[warp][e + 1] : s_list[warp][e]};
-        FwdPre pre[2][NP];
-        uint32_t need = 0;
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const float4 A = s_a[jj[u]];
-          const float4 B = s_b[jj[u]];
-          const float dx = esub(A.x, pcx);
-          const float t1 = emul(emul(A.z, dx), dx);
-          const float t2 = emul(A.w, dx);
-#pragma unroll
-          for (int k = 0; k < NP; ++k) {
-            FwdPre& q = pre[u][k];
-            const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
-            q.sg = sigma2(t1, t2, dy, B.x);
-            q.l0 = !(q.sg.x > B.y);
-            q.l1 = !(q.sg.y > B.y);
-            q.opac = B.z;
-            if (__any_sync(0xffffffffu, (q.l0 && !done[2 * k]) || (q.l1 && !done[2 * k + 1])) && (u == 0 || two))
-              need |= 1u << (u * NP + k);
-          }
-        }
-        // blend_alpha_of (sigma >= 0 and alpha >= 1/255) and the blend of
-        // entry u, pair k. A pixel that does not take the Gaussian blends
-        // with alpha 0, which leaves its colour and transmittance bit for bit
-        // unchanged.
-        auto alpha = [&](FwdPre& q) {
-          const float2 og = mul2(f2(q.opac), blend_exp2(q.sg));
-          q.ax = fminf(0.999f, og.x);
-          q.ay = fminf(0.999f, og.y);
-          q.c0 = q.l0 && q.sg.x >= 0.f && q.ax >= (float)(1.0 / 255.0);
-          q.c1 = q.l1 && q.sg.y >= 0.f && q.ay >= (float)(1.0 / 255.0);
-        };
-        auto blend = [&](int u, int k) {
-          const FwdPre& q = pre[u][k];
-          const bool c0 = q.c0 && !done[2 * k], c1 = q.c1 && !done[2 * k + 1];
-          if (!(c0 || c1)) return;
-          const uint32_t j = jj[u];
-          const float2 am = make_float2(c0 ? q.ax : 0.f, c1 ? q.ay : 0.f);
-          const float4 Cc = s_c[j];
-          const float2 w = mul2(am, T[k]);
-          C0[k] = fma2(f2(Cc.x), w, C0[k]);  // blend_accum; Cc was clamped at staging
-          C1[k] = fma2(f2(Cc.y), w, C1[k]);
-          C2[k] = fma2(f2(Cc.z), w, C2[k]);
-          T[k] = mul2(T[k], add2(f2(1.f), neg2(am)));
-          s_hit[warp][j] = 1;
-          if (c0) {
-            last[2 * k] = b0 + j + 1;
-            ++nc[2 * k];
-            if (T[k].x < 1e-4f) done[2 * k] = true;
-          }
-          if (c1) {
-            last[2 * k + 1] = b0 + j + 1;
-            ++nc[2 * k + 1];
-            if (T[k].y < 1e-4f) done[2 * k + 1] = true;
-          }
-        };
-        static_assert(NP == 1, "the forward runs one pixel pair per lane");
-        if (need == 3u) {
-          alpha(pre[0][0]);
-          alpha(pre[1][0]);
-          blend(0, 0);
-          blend(1, 0);
-        } else if (need == 1u) {
-          alpha(pre[0][0]);
-          blend(0, 0);
-        } else if (need == 2u) {
-          alpha(pre[1][0]);
-          blend(1, 0);
-        }
-        all_done = true;
-#pragma unroll
-        for (int q = 0; q < PPL; ++q) all_done = all_done && done[q];
-        if (__all_sync(0xffffffffu, all_done)) break;
+  #pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      const uint32_t py = pyb + 4 * q;
+      last[q] = nc[q] = 0;
+      done[q] = !(px < vd.w && py < vd.h);
+      all_done = all_done && done[q];
+    }
+    for (uint32_t b0 = s0; b0 < s1; b0 += BATCH) {
+      const uint32_t nb = min((uint32_t)BATCH, s1 - b0);
+      __syncthreads();
+      for (uint32_t j = threadIdx.x; j < nb; j += NT) {
+        const uint32_t c = vals[b0 + j] & vmask;
+        float4 A, B, Cc;
+        s_mask[j] = (uint8_t)stage_one<TW, PPL, NW>(rec, c, tx0, ty0, A, B, Cc);
+        s_a[j] = A;
+        s_b[j] = B;
+        s_c[j] = Cc;
+        s_cidx[j] = c;
+  #pragma unroll
+        for (int w = 0; w < NW; ++w) s_hit[w][j] = 0;
       }
+      __syncthreads();
+      if (!__all_sync(0xffffffffu, all_done)) {
+        const int cnt = build_list(s_mask, nb, 1u << warp, lane, s_list[warp]);
+        // Entries go two at a time: the sigma, cut test, exponential and
+        // contribution test of both (independent of the pixel state) form one
+        // straight-line block whose chains interleave; the blends then apply
+        // in list order, the second gated by the pixel state the first left.
+        for (int e = 0; e < cnt; e += 2) {
+          const bool two = e + 1 < cnt;  // warp-uniform
+          const uint32_t jj[2] = {s_list[warp][e], two ? s_list[warp][e + 1] : s_list[warp][e]};
+          FwdPre pre[2][NP];
+          uint32_t need = 0;
+  #pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const float4 A = s_a[jj[u]];
+            const float4 B = s_b[jj[u]];
+            const float dx = esub(A.x, pcx);
+            const float t1 = emul(emul(A.z, dx), dx);
+            const float t2 = emul(A.w, dx);
+  #pragma unroll
+            for (int k = 0; k < NP; ++k) {
+              FwdPre& q = pre[u][k];
+              const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
+              q.sg = sigma2(t1, t2, dy, B.x);
+              q.l0 = !(q.sg.x > B.y);
+              q.l1 = !(q.sg.y > B.y);
+              q.opac = B.z;
+              if (__any_sync(0xffffffffu, (q.l0 && !done[2 * k]) || (q.l1 && !done[2 * k + 1])) && (u == 0 || two))
+                need |= 1u << (u * NP + k);
+            }
+          }
+          // blend_alpha_of (sigma >= 0 and alpha >= 1/255) and the blend of
+          // entry u, pair k. A pixel that does not take the Gaussian blends
+          // with alpha 0, which leaves its colour and transmittance bit for bit
+          // unchanged.
+          auto alpha = [&](FwdPre& q) {
+            const float2 og = mul2(f2(q.opac), blend_exp2(q.sg));
+            q.ax = fminf(0.999f, og.x);
+            q.ay = fminf(0.999f, og.y);
+            q.c0 = q.l0 && q.sg.x >= 0.f && q.ax >= (float)(1.0 / 255.0);
+            q.c1 = q.l1 && q.sg.y >= 0.f && q.ay >= (float)(1.0 / 255.0);
+          };
+          auto blend = [&](int u, int k) {
+            const FwdPre& q = pre[u][k];
+            const bool c0 = q.c0 && !done[2 * k], c1 = q.c1 && !done[2 * k + 1];
+            if (!(c0 || c1)) return;
+            const uint32_t j = jj[u];
+            const float2 am = make_float2(c0 ? q.ax : 0.f, c1 ? q.ay : 0.f);
+            const float4 Cc = s_c[j];
+            const float2 w = mul2(am, T[k]);
+            C0[k] = fma2(f2(Cc.x), w, C0[k]);  // blend_accum; Cc was clamped at staging
+            C1[k] = fma2(f2(Cc.y), w, C1[k]);
+            C2[k] = fma2(f2(Cc.z), w, C2[k]);
+            T[k] = mul2(T[k], add2(f2(1.f), neg2(am)));
+            s_hit[warp][j] = 1;
+            if (c0) {
+              last[2 * k] = b0 + j + 1;
+              ++nc[2 * k];
+              if (T[k].x < 1e-4f) done[2 * k] = true;
+            }
+            if (c1) {
+              last[2 * k + 1] = b0 + j + 1;
+              ++nc[2 * k + 1];
+              if (T[k].y < 1e-4f) done[2 * k + 1] = true;
+            }
+          };
+          static_assert(NP == 1, "the forward runs one pixel pair per lane");
+          if (need == 3u) {
+            alpha(pre[0][0]);
+            alpha(pre[1][0]);
+            blend(0, 0);
+            blend(1, 0);
+          } else if (need == 1u) {
+            alpha(pre[0][0]);
+            blend(0, 0);
+          } else if (need == 2u) {
+            alpha(pre[1][0]);
+            blend(1, 0);
+          }
+          all_done = true;
+  #pragma unroll
+          for (int q = 0; q < PPL; ++q) all_done = all_done && done[q];
+          if (__all_sync(0xffffffffu, all_done)) break;
+        }
+      }
+      __syncthreads();
+      for (uint32_t j = threadIdx.x; j < nb; j += NT) {
+        uint32_t bits = 0;
+  #pragma unroll
+        for (int w = 0; w < NW; ++w) bits |= (uint32_t)s_hit[w][j] << w;
+        hitw[b0 + j] = (uint8_t)bits;  // bit w: the 8x8 block of warp w
+        if (bits) vis[s_cidx[j]] = 1;
+      }
+      if (__syncthreads_and(all_done)) break;
     }
+    float4* out = reinterpret_cast<float4*>(a.out_rgba) + vd.pix_base;
+  #pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      const uint32_t py = pyb + 4 * q;
+      if (!(px < vd.w && py < vd.h)) continue;
+      const size_t pix = (size_t)py * vd.w + px;
+      const int k = q / 2;
+      const float Tq = (q & 1) ? T[k].y : T[k].x;
+      const float c0 = (q & 1) ? C0[k].y : C0[k].x;
+      const float c1 = (q & 1) ? C1[k].y : C1[k].x;
+      const float c2 = (q & 1) ? C2[k].y : C2[k].x;
+      out[pix] = make_float4(c0 + Tq * a.bg[0], c1 + Tq * a.bg[1], c2 + Tq * a.bg[2], 1.f - Tq);
+      slice(a.b.tfinal, a.b.Pcap, v)[pix] = Tq;
+      slice(a.b.last, a.b.Pcap, v)[pix] = last[q];
+      slice(a.b.ncontrib, a.b.Pcap, v)[pix] = nc[q];
+      slice(a.b.nvisit, a.b.Pcap, v)[pix] = (done[q] ? last[q] : s1) - s0;
+    }
+    // The backward's cost of this item: list entries up to the tile's
+    // largest last contributor.
+    uint32_t ml = 0;
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) ml = max(ml, last[q]);
+    ml = __reduce_max_sync(0xffffffffu, ml);
+    if (lane == 0 && ml) atomicMax(&s_work, ml);
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += NT) {
-      uint32_t bits = 0;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) bits |= (uint32_t)s_hit[w][j] << w;
-      hitw[b0 + j] = (uint8_t)bits;  // bit w: the 8x8 block of warp w
-      if (bits) vis[s_cidx[j]] = 1;
+    if (threadIdx.x == 0) {
+      a.b.sched_work[item] = s_work > s0 ? s_work - s0 : 0u;
+      s_work = 0u;
     }
-    if (__syncthreads_and(all_done)) break;
-  }
-  float4* out = reinterpret_cast<float4*>(a.out_rgba) + vd.pix_base;
-#pragma unroll
-  for (int q = 0; q < PPL; ++q) {
-    const uint32_t py = pyb + 4 * q;
-    if (!(px < vd.w && py < vd.h)) continue;
-    const size_t pix = (size_t)py * vd.w + px;
-    const int k = q / 2;
-    const float Tq = (q & 1) ? T[k].y : T[k].x;
-    const float c0 = (q & 1) ? C0[k].y : C0[k].x;
-    const float c1 = (q & 1) ? C1[k].y : C1[k].x;
-    const float c2 = (q & 1) ? C2[k].y : C2[k].x;
-    out[pix] = make_float4(c0 + Tq * a.bg[0], c1 + Tq * a.bg[1], c2 + Tq * a.bg[2], 1.f - Tq);
-    slice(a.b.tfinal, a.b.Pcap, v)[pix] = Tq;
-    slice(a.b.last, a.b.Pcap, v)[pix] = last[q];
-    slice(a.b.ncontrib, a.b.Pcap, v)[pix] = nc[q];
-    slice(a.b.nvisit, a.b.Pcap, v)[pix] = (done[q] ? last[q] : s1) - s0;
   }
 }
 
@@ -578,201 +662,205 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   __shared__ uint16_t s_list[NW][BATCH];
   __shared__ float4 s_part[NW][BATCH][3];      // written by the warps whose bit is set
   __shared__ uint32_t s_max;
-  const uint32_t item = blockIdx.x;
-  const uint32_t v = find_view(a.vs, item);
-  const ViewDesc& vd = a.vs.views[v];
-  const uint32_t t = item - vd.tile_base;
-  const uint32_t tx = t % vd.tiles_x, ty = t / vd.tiles_x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t px = tx * TW + WarpBlock<TW, PPL>::x0(warp) + (lane & 7);
-  const uint32_t pyb = ty * TH + WarpBlock<TW, PPL>::y0(warp) + (lane >> 3);
-  const float pcx = (float)px + 0.5f;
-  const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
-  const uint32_t s0 = ranges[2 * t];
-  const uint32_t* vals = isect_index_src(a.b, v);
-  const uint32_t vmask = isect_index_mask(a.b);
-  const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
-  const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
-  float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
-  float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
-  BwdPair pp[NP];
-  uint32_t mylast = 0;
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    load_bwd_pair(a, vd, v, px, pyb + 8 * k, pp[k]);
-    mylast = max(mylast, max(pp[k].last0, pp[k].last1));
-  }
-  if (threadIdx.x == 0) s_max = 0;
-  __syncthreads();
-  const uint32_t wmax = __reduce_max_sync(0xffffffffu, mylast);
-  if (lane == 0) atomicMax(&s_max, wmax);
-  __syncthreads();
-  const uint32_t smax = s_max;
-  const int slot = reduce12_slot(lane);                          // the gradient value this lane ends with
-  const bool writer = (lane & 1) == 0 && !((lane & 2) && (lane & 4));  // one lane per value
-  uint32_t wsel = 0;  // the forward blocks inside this warp's block
-#pragma unroll
-  for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
-  auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
-  // List entries [lo, hi) of a batch into registers.
-  uint32_t pc[kSI], ph[kSI];
-  auto fetch = [&](uint32_t lo, uint32_t hi) {
-#pragma unroll
-    for (int it = 0; it < kSI; ++it) {
-      const uint32_t s = lo + threadIdx.x + it * NT;
-      const bool ok = threadIdx.x + it * NT < (uint32_t)BATCH && s < hi;
-      ph[it] = ok ? hitw[s] : 0u;
-      pc[it] = ok ? (vals[s] & vmask) : 0u;
+  __shared__ uint32_t s_item;
+  for (uint32_t round = 0;; ++round) {
+    const uint32_t item = next_item(a, round, &s_item);
+    if (item == kNoItem) break;
+    const uint32_t v = find_view(a.vs, item);
+    const ViewDesc& vd = a.vs.views[v];
+    const uint32_t t = item - vd.tile_base;
+    const uint32_t tx = t % vd.tiles_x, ty = t / vd.tiles_x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t px = tx * TW + WarpBlock<TW, PPL>::x0(warp) + (lane & 7);
+    const uint32_t pyb = ty * TH + WarpBlock<TW, PPL>::y0(warp) + (lane >> 3);
+    const float pcx = (float)px + 0.5f;
+    const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
+    const uint32_t s0 = ranges[2 * t];
+    const uint32_t* vals = isect_index_src(a.b, v);
+    const uint32_t vmask = isect_index_mask(a.b);
+    const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
+    const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
+    float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
+    float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
+    BwdPair pp[NP];
+    uint32_t mylast = 0;
+  #pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      load_bwd_pair(a, vd, v, px, pyb + 8 * k, pp[k]);
+      mylast = max(mylast, max(pp[k].last0, pp[k].last1));
     }
-  };
-  // Masks, indices and record copies of the fetched batch [lo, hi) into
-  // buffer `buf`; one commit group per call.
-  auto issue = [&](uint32_t lo, uint32_t hi, int buf) {
-#pragma unroll
-    for (int it = 0; it < kSI; ++it) {
-      const uint32_t j = threadIdx.x + it * NT;
-      if (j < (uint32_t)BATCH && lo + j < hi) {
-        s_mask[buf][j] = (uint8_t)ph[it];  // the forward's 8x8 block bits
-        if (ph[it]) {
-          s_cidx[buf][j] = pc[it];
-          const float4* r = rec + (size_t)pc[it] * 3;
-          cp_async16(&s_rec[buf][j][0], r);
-          cp_async16(&s_rec[buf][j][1], r + 1);
-          cp_async16(&s_rec[buf][j][2], r + 2);
-        }
-      }
-    }
-    cp_async_commit();
-  };
-  uint32_t be = smax, bs = be > s0 ? batch_lo(be) : s0;
-  if (be > s0) {
-    fetch(bs, be);
-    issue(bs, be, 0);
-  }
-  uint32_t nbe = bs, nbs = nbe > s0 ? batch_lo(nbe) : s0;
-  if (nbe > s0) fetch(nbs, nbe);
-  int buf = 0;
-  while (be > s0) {
-    const uint32_t nb = be - bs;
-    if (nbe > s0)
-      issue(nbs, nbe, buf ^ 1);
-    else
-      cp_async_commit();
-    const uint32_t n2e = nbs, n2s = n2e > s0 ? batch_lo(n2e) : s0;
-    if (n2e > s0) fetch(n2s, n2e);
-    cp_async_wait1();  // this thread's copies of the current batch have landed
+    if (threadIdx.x == 0) s_max = 0;
     __syncthreads();
-    if (bs < wmax) {
-      const int cnt = build_list(s_mask[buf], nb, wsel, lane, s_list[warp]);
-      for (int e = cnt - 1; e >= 0; --e) {
-        const uint32_t j = s_list[warp][e];
-        const uint32_t s = bs + j;
-        const float4 r0 = s_rec[buf][j][0], r1 = s_rec[buf][j][1], r2 = s_rec[buf][j][2];
-        const float4 A = make_float4(r0.x, r0.y, r0.z, 2.f * r0.w);  // 2b is exact
-        const float4 B = make_float4(r1.x, r2.y + kRejectMargin, r1.y, 0.f);
-        const float4 Cc = make_float4(r1.z, r1.w, r2.x, 0.f);
-        const float dx = esub(A.x, pcx);
-        const float t1 = emul(emul(A.z, dx), dx);
-        const float t2 = emul(A.w, dx);
-        const float cb = 0.5f * A.w;
-        const float adx = A.z * dx, bdx = cb * dx;
-        BwdAcc acc;
-        acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.op = f2(0.f);
-        acc.ax = acc.ay = 0.f;
-        acc.n = 0u;
-        const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
-        // The pairs of this warp whose 8x8 block had a pixel take the
-        // Gaussian in the forward (the others contribute nothing here).
-        const uint32_t mraw = s_mask[buf][j];
-        uint32_t need = 0;
-#pragma unroll
-        for (int k = 0; k < NP; ++k)
-          if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) need |= 1u << k;
-        // The needed pairs run as one straight-line block (need is
-        // warp-uniform), so that their independent chains interleave.
-        auto rest = [&](int k) {
-          const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
-          const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
-          const float2 cpv =
-              fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
-          bwd_pair_rest<REF>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
-        };
-        if constexpr (NP == 2) {
-          if (need == 3u) {
-            rest(0);
-            rest(1);
-          } else if (need == 1u) {
-            rest(0);
-          } else if (need == 2u) {
-            rest(1);
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, mylast);
+    if (lane == 0) atomicMax(&s_max, wmax);
+    __syncthreads();
+    const uint32_t smax = s_max;
+    const int slot = reduce12_slot(lane);                          // the gradient value this lane ends with
+    const bool writer = (lane & 1) == 0 && !((lane & 2) && (lane & 4));  // one lane per value
+    uint32_t wsel = 0;  // the forward blocks inside this warp's block
+  #pragma unroll
+    for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
+    auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
+    // List entries [lo, hi) of a batch into registers.
+    uint32_t pc[kSI], ph[kSI];
+    auto fetch = [&](uint32_t lo, uint32_t hi) {
+  #pragma unroll
+      for (int it = 0; it < kSI; ++it) {
+        const uint32_t s = lo + threadIdx.x + it * NT;
+        const bool ok = threadIdx.x + it * NT < (uint32_t)BATCH && s < hi;
+        ph[it] = ok ? hitw[s] : 0u;
+        pc[it] = ok ? (vals[s] & vmask) : 0u;
+      }
+    };
+    // Masks, indices and record copies of the fetched batch [lo, hi) into
+    // buffer `buf`; one commit group per call.
+    auto issue = [&](uint32_t lo, uint32_t hi, int buf) {
+  #pragma unroll
+      for (int it = 0; it < kSI; ++it) {
+        const uint32_t j = threadIdx.x + it * NT;
+        if (j < (uint32_t)BATCH && lo + j < hi) {
+          s_mask[buf][j] = (uint8_t)ph[it];  // the forward's 8x8 block bits
+          if (ph[it]) {
+            s_cidx[buf][j] = pc[it];
+            const float4* r = rec + (size_t)pc[it] * 3;
+            cp_async16(&s_rec[buf][j][0], r);
+            cp_async16(&s_rec[buf][j][1], r + 1);
+            cp_async16(&s_rec[buf][j][2], r + 2);
           }
-        } else {
-#pragma unroll
+        }
+      }
+      cp_async_commit();
+    };
+    uint32_t be = smax, bs = be > s0 ? batch_lo(be) : s0;
+    if (be > s0) {
+      fetch(bs, be);
+      issue(bs, be, 0);
+    }
+    uint32_t nbe = bs, nbs = nbe > s0 ? batch_lo(nbe) : s0;
+    if (nbe > s0) fetch(nbs, nbe);
+    int buf = 0;
+    while (be > s0) {
+      const uint32_t nb = be - bs;
+      if (nbe > s0)
+        issue(nbs, nbe, buf ^ 1);
+      else
+        cp_async_commit();
+      const uint32_t n2e = nbs, n2s = n2e > s0 ? batch_lo(n2e) : s0;
+      if (n2e > s0) fetch(n2s, n2e);
+      cp_async_wait1();  // this thread's copies of the current batch have landed
+      __syncthreads();
+      if (bs < wmax) {
+        const int cnt = build_list(s_mask[buf], nb, wsel, lane, s_list[warp]);
+        for (int e = cnt - 1; e >= 0; --e) {
+          const uint32_t j = s_list[warp][e];
+          const uint32_t s = bs + j;
+          const float4 r0 = s_rec[buf][j][0], r1 = s_rec[buf][j][1], r2 = s_rec[buf][j][2];
+          const float4 A = make_float4(r0.x, r0.y, r0.z, 2.f * r0.w);  // 2b is exact
+          const float4 B = make_float4(r1.x, r2.y + kRejectMargin, r1.y, 0.f);
+          const float4 Cc = make_float4(r1.z, r1.w, r2.x, 0.f);
+          const float dx = esub(A.x, pcx);
+          const float t1 = emul(emul(A.z, dx), dx);
+          const float t2 = emul(A.w, dx);
+          const float cb = 0.5f * A.w;
+          const float adx = A.z * dx, bdx = cb * dx;
+          BwdAcc acc;
+          acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.op = f2(0.f);
+          acc.ax = acc.ay = 0.f;
+          acc.n = 0u;
+          const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
+          // The pairs of this warp whose 8x8 block had a pixel take the
+          // Gaussian in the forward (the others contribute nothing here).
+          const uint32_t mraw = s_mask[buf][j];
+          uint32_t need = 0;
+  #pragma unroll
           for (int k = 0; k < NP; ++k)
-            if (need & (1u << k)) rest(k);
+            if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) need |= 1u << k;
+          // The needed pairs run as one straight-line block (need is
+          // warp-uniform), so that their independent chains interleave.
+          auto rest = [&](int k) {
+            const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
+            const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
+            const float2 cpv =
+                fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
+            bwd_pair_rest<REF>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
+          };
+          if constexpr (NP == 2) {
+            if (need == 3u) {
+              rest(0);
+              rest(1);
+            } else if (need == 1u) {
+              rest(0);
+            } else if (need == 2u) {
+              rest(1);
+            }
+          } else {
+  #pragma unroll
+            for (int k = 0; k < NP; ++k)
+              if (need & (1u << k)) rest(k);
+          }
+          const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
+          float x[12];
+          x[0] = adx * M0 + cb * M1;
+          x[1] = bdx * M0 + B.x * M1;
+          x[2] = (0.5f * dx * dx) * M0;
+          x[3] = dx * M1;
+          x[4] = 0.5f * M2;
+          x[5] = acc.cr.x + acc.cr.y;
+          x[6] = acc.cg.x + acc.cg.y;
+          x[7] = acc.cb.x + acc.cb.y;
+          x[8] = acc.op.x + acc.op.y;
+          x[9] = acc.ax;
+          x[10] = acc.ay;
+          x[11] = (float)acc.n;
+          float r = warp_reduce_scatter12(x, lane);
+          // v_rgb is zero for a channel whose raw colour is negative.
+          if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
+          float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
+          if (writer) sp[slot] = r;
         }
-        const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
-        float x[12];
-        x[0] = adx * M0 + cb * M1;
-        x[1] = bdx * M0 + B.x * M1;
-        x[2] = (0.5f * dx * dx) * M0;
-        x[3] = dx * M1;
-        x[4] = 0.5f * M2;
-        x[5] = acc.cr.x + acc.cr.y;
-        x[6] = acc.cg.x + acc.cg.y;
-        x[7] = acc.cb.x + acc.cb.y;
-        x[8] = acc.op.x + acc.op.y;
-        x[9] = acc.ax;
-        x[10] = acc.ay;
-        x[11] = (float)acc.n;
-        float r = warp_reduce_scatter12(x, lane);
-        // v_rgb is zero for a channel whose raw colour is negative.
-        if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
-        float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
-        if (writer) sp[slot] = r;
       }
-    }
-    __syncthreads();
-    for (uint32_t q = threadIdx.x; q < nb * 3; q += NT) {
-      const uint32_t j = q / 3, k = q % 3;
-      const uint32_t m = hit_bits_for<TW, TH, PPL>(s_mask[buf][j]);  // warps that wrote a slot
-      float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-      bool any = false;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        if (!((m >> w) & 1u)) continue;
-        const float4 g = s_part[w][j][k];
-        if (!any) {
-          f = g;
-          any = true;
-        } else {
-          f.x = f.x + g.x;
-          f.y = f.y + g.y;
-          f.z = f.z + g.z;
-          f.w = f.w + g.w;
+      __syncthreads();
+      for (uint32_t q = threadIdx.x; q < nb * 3; q += NT) {
+        const uint32_t j = q / 3, k = q % 3;
+        const uint32_t m = hit_bits_for<TW, TH, PPL>(s_mask[buf][j]);  // warps that wrote a slot
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool any = false;
+  #pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          if (!((m >> w) & 1u)) continue;
+          const float4 g = s_part[w][j][k];
+          if (!any) {
+            f = g;
+            any = true;
+          } else {
+            f.x = f.x + g.x;
+            f.y = f.y + g.y;
+            f.z = f.z + g.z;
+            f.w = f.w + g.w;
+          }
+        }
+        if (a.det) {
+          reinterpret_cast<float4*>(part + (size_t)(bs + j) * 12)[k] = f;
+        } else if (f.x != 0.f || f.y != 0.f || f.z != 0.f || f.w != 0.f) {
+          atomicAdd(sgrad + (size_t)s_cidx[buf][j] * 3 + k, f);
         }
       }
-      if (a.det) {
-        reinterpret_cast<float4*>(part + (size_t)(bs + j) * 12)[k] = f;
-      } else if (f.x != 0.f || f.y != 0.f || f.z != 0.f || f.w != 0.f) {
-        atomicAdd(sgrad + (size_t)s_cidx[buf][j] * 3 + k, f);
-      }
+      __syncthreads();  // the next batch's copies reuse this buffer
+      be = bs;
+      bs = nbs;
+      nbe = n2e;
+      nbs = n2s;
+      buf ^= 1;
     }
-    __syncthreads();  // the next batch's copies reuse this buffer
-    be = bs;
-    bs = nbs;
-    nbe = n2e;
-    nbs = n2s;
-    buf ^= 1;
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may outlive the block
-  // Deterministic mode: list entries of this tile that no pixel reached keep
-  // zero partial records.
-  if (a.det) {
-    const uint32_t s1 = ranges[2 * t + 1];
-    for (uint32_t s = smax > s0 ? smax : s0; s + threadIdx.x < s1; s += NT) {
-      float4* p4 = reinterpret_cast<float4*>(part + (size_t)(s + threadIdx.x) * 12);
-      p4[0] = p4[1] = p4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may outlive the block
+    // Deterministic mode: list entries of this tile that no pixel reached keep
+    // zero partial records.
+    if (a.det) {
+      const uint32_t s1 = ranges[2 * t + 1];
+      for (uint32_t s = smax > s0 ? smax : s0; s + threadIdx.x < s1; s += NT) {
+        float4* p4 = reinterpret_cast<float4*>(part + (size_t)(s + threadIdx.x) * 12);
+        p4[0] = p4[1] = p4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
   }
 }
@@ -787,40 +875,60 @@ inline int pick_batch(uint32_t want, int dflt) {
   return want <= 64 ? 64 : (want <= 128 ? 128 : 256);
 }
 
-template <int TW, int TH, int PPL>
-cudaError_t launch_fwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
-  constexpr int NT = TW * TH / PPL;
-  switch (pick_batch(batch, 128)) {
-    case 64: raster_fwd_kernel<TW, TH, PPL, 64><<<items, NT, 0, st>>>(a); break;
-    case 128: raster_fwd_kernel<TW, TH, PPL, 128><<<items, NT, 0, st>>>(a); break;
-    default: raster_fwd_kernel<TW, TH, PPL, 256><<<items, NT, 0, st>>>(a); break;
+// Launches kernel over the launch's work items: one CTA per item (grid
+// schedule), or as many CTAs as the SMs hold at once (persistent schedule;
+// the residency of each instantiation is looked up once).
+template <void (*Kernel)(RasterArgs)>
+cudaError_t launch_items(int threads, const RasterArgs& a, int num_sms, cudaStream_t st) {
+  uint32_t grid = a.vs.total_tiles;
+  if (a.vs.persistent) {
+    static int per_sm = 0;  // one per kernel instantiation
+    if (per_sm <= 0) {
+      int n = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, Kernel, threads, 0) != cudaSuccess || n < 1) {
+        (void)cudaGetLastError();
+        n = 1;
+      }
+      per_sm = n;
+    }
+    grid = std::min<uint32_t>(grid, (uint32_t)per_sm * (uint32_t)std::max(num_sms, 1));
   }
+  Kernel<<<grid, threads, 0, st>>>(a);
   return cudaGetLastError();
 }
+
+template <int TW, int TH, int PPL>
+cudaError_t launch_fwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
+  constexpr int NT = TW * TH / PPL;
+  switch (pick_batch(batch, 128)) {
+    case 64: return launch_items<raster_fwd_kernel<TW, TH, PPL, 64>>(NT, a, num_sms, st);
+    case 128: return launch_items<raster_fwd_kernel<TW, TH, PPL, 128>>(NT, a, num_sms, st);
+    default: return launch_items<raster_fwd_kernel<TW, TH, PPL, 256>>(NT, a, num_sms, st);
+  }
+}
 template <int TW, int TH, int PPL, bool REF>
-cudaError_t launch_bwd_mode(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
+cudaError_t launch_bwd_mode(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
   constexpr int NT = TW * TH / PPL;
   constexpr int kMaxBatch = NT / 32 >= 2 ? 128 : 256;
   int b = pick_batch(batch, 64);
   if (b > kMaxBatch) b = kMaxBatch;
   switch (b) {
-    case 64: raster_bwd_kernel<TW, TH, PPL, 64, REF><<<items, NT, 0, st>>>(a); break;
-    case 128: raster_bwd_kernel<TW, TH, PPL, 128, REF><<<items, NT, 0, st>>>(a); break;
-    default: raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128), REF><<<items, NT, 0, st>>>(a); break;
+    case 64: return launch_items<raster_bwd_kernel<TW, TH, PPL, 64, REF>>(NT, a, num_sms, st);
+    case 128: return launch_items<raster_bwd_kernel<TW, TH, PPL, 128, REF>>(NT, a, num_sms, st);
+    default:
+      return launch_items<raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128), REF>>(NT, a, num_sms, st);
   }
-  return cudaGetLastError();
 }
 template <int TW, int TH, int PPL>
-cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t items, uint32_t batch, cudaStream_t st) {
-  return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, items, batch, st)
-                    : launch_bwd_mode<TW, TH, PPL, false>(a, items, batch, st);
+cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
+  return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, batch, num_sms, st)
+                    : launch_bwd_mode<TW, TH, PPL, false>(a, batch, num_sms, st);
 }
 
 }  // namespace
 
 cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, float* out_rgba, const Scratch& s,
                               cudaStream_t st) {
-  (void)s;
   RasterArgs a{};
   a.vs = vs;
   a.b = b;
@@ -831,15 +939,19 @@ cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, fl
   cudaError_t e = cudaMemsetAsync(b.visible_c, 0, b.Vcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, kFwdPPL>(a, vs.total_tiles, vs.batch, st);
+  if (vs.persistent) {
+    sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_fwd_shape<16, 16, kFwdPPL>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_fwd_shape<8, 8, kFwdPPL>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_fwd_shape<32, 8, kFwdPPL>(a, vs.batch, s.num_sms, st);
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, const float* v_rgba, int ref_mode,
                               int deterministic, const Scratch& s, cudaStream_t st) {
-  (void)s;
   RasterArgs a{};
   a.vs = vs;
   a.b = b;
@@ -854,9 +966,14 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     if (e != cudaSuccess) return e;
   }
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.total_tiles, vs.batch, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.total_tiles, vs.batch, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.total_tiles, vs.batch, st);
+  if (vs.persistent) {
+    sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.batch, s.num_sms, st);
   return cudaErrorInvalidValue;
 }
 

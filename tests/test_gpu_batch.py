@@ -7,7 +7,9 @@ Every view of the batch is bit-exact against the oracle's single-view
 forward; the batched backward equals the sum of the per-view oracle
 adjoints; every tile shape and raster batch size gives the same bit-exact
 forward; the autotuner returns a runnable configuration whose forward is
-again bit-exact."""
+again bit-exact; the persistent cost-ordered raster schedule and the
+one-CTA-per-tile grid give the same forward bit for bit, gradients within
+the parity bar, and bitwise equal gradients in deterministic mode."""
 import numpy as np
 import pytest
 
@@ -29,13 +31,14 @@ def _dev(scene):
     return host_splats_to_device(scene)
 
 
-def test_uneven_batch_forward_and_backward(gsr_ctx_factory):
+@pytest.mark.parametrize("schedule", ["persistent", "grid"])
+def test_uneven_batch_forward_and_backward(gsr_ctx_factory, schedule):
     import torch
 
     sc = _scene()
     nv = len(sc.cameras)
     counts = []
-    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=max(w * h for w, h in RES))
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=max(w * h for w, h in RES), schedule=schedule)
     splats = _dev(sc)
     _, g = run_gpu_forward(ctx, splats, sc.cameras)
     ups = [S.upstream_grad(c.height, c.width, seed=v) for v, c in enumerate(sc.cameras)]
@@ -85,3 +88,37 @@ def test_autotune_picks_a_runnable_configuration(gsr_ctx_factory):
     _, g = run_gpu_forward(ctx, splats, sc.cameras)
     for v in (0, nv - 1):
         assert_forward_parity(g[v], oracle_forward(sc, sc.cameras[v], tile=res["tile"]))
+
+
+@pytest.mark.parametrize("tile", [(16, 16), (8, 8), (32, 8)])
+def test_schedules_agree(gsr_ctx_factory, tile):
+    """Persistent and grid schedules: identical images and per-pixel state,
+    gradients within the parity bar of each other's oracle, and in
+    deterministic mode bitwise identical gradients."""
+    import torch
+
+    sc = _scene()
+    nv = len(sc.cameras)
+    pmax = max(w * h for w, h in RES)
+    splats = _dev(sc)
+    ups = torch.as_tensor(np.concatenate([S.upstream_grad(c.height, c.width, seed=v).reshape(-1)
+                                          for v, c in enumerate(sc.cameras)]), device="cuda")
+    out = {}
+    for det in (False, True):
+        for schedule in ("persistent", "grid"):
+            ctx = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=pmax, tile=tile, schedule=schedule,
+                                  deterministic=det)
+            _, g = run_gpu_forward(ctx, splats, sc.cameras)
+            gr = ctx.render_backward(splats, ups)
+            torch.cuda.synchronize()
+            out[(det, schedule)] = (g, {k: gr[k].cpu().numpy() for k in ("v_transforms", "v_sh", "v_raw_opacity")})
+            ctx.close()
+    for det in (False, True):
+        ga, gb = out[(det, "persistent")][0], out[(det, "grid")][0]
+        for v in range(nv):
+            for k in ("image", "tfinal", "last", "ncontrib", "nvisit", "hit_blocks", "isect_vals", "visible"):
+                np.testing.assert_array_equal(ga[v][k], gb[v][k], err_msg=f"{k} view {v}")
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        np.testing.assert_array_equal(out[(True, "persistent")][1][k], out[(True, "grid")][1][k])
+        a, b = out[(False, "persistent")][1][k], out[(False, "grid")][1][k]
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), k
