@@ -391,7 +391,7 @@ def _render_op_line(args, name, sc, contexts, workload, dtype, extra=None):
             ctx.render_backward(splats, up, stats=True)
 
         ms = _time_device(step, args.steps, args.warmup)
-        res[label] = {"ms_per_view": ms}
+        res[label] = {"ms_per_view": ms, "stages_ms": stage_profile(ctx, step)}
         if first is None:
             first = (label, ctx, splats, ms)
         else:

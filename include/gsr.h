@@ -57,8 +57,10 @@ enum { GSR_ADJOINT_EXACT = 0, GSR_ADJOINT_REFERENCE = 1 };
  * backward by the list entries up to the tile's last contributor, which the
  * forward records), so the longest tiles start first and the launch ends
  * without a tail of long tiles. GRID: one CTA per item in view and tile
- * order, scheduled by the hardware. The results are the same; with float
- * atomics (deterministic = 0) the gradient sums may differ in the last bits. */
+ * order, scheduled by the hardware. DEFAULT: the backward persistent, the
+ * forward as a grid (the forward's cost, its entries up to saturation, is
+ * not known before it runs). The results are the same; with float atomics
+ * (deterministic = 0) the gradient sums may differ in the last bits. */
 enum { GSR_SCHEDULE_DEFAULT = 0, GSR_SCHEDULE_PERSISTENT = 1, GSR_SCHEDULE_GRID = 2 };
 
 /* Context configuration. Replaces the rasterizer fields of RustGS's
@@ -77,7 +79,7 @@ typedef struct gsr_config {
   int32_t fp64_conic;      /* 1: 2x2 covariance inversion in FP64 */
   uint64_t max_splats;     /* capacity in Gaussians */
   uint32_t max_views;      /* views per forward (1) */
-  uint32_t schedule;       /* GSR_SCHEDULE_*: raster work scheduling (default: persistent) */
+  uint32_t schedule;       /* GSR_SCHEDULE_*: raster work scheduling */
   uint64_t max_pixels;     /* capacity in pixels per view */
   uint64_t max_isects;     /* tile intersections per view (0: 16 * max_splats, at least 2^20) */
 } gsr_config;

@@ -53,12 +53,13 @@ struct FwdBufs {
 };
 
 // The compact index of intersection s (packed keys or pairs).
-__device__ __forceinline__ const uint32_t* isect_index_src(const FwdBufs& b, uint32_t v) {
+__host__ __device__ __forceinline__ const uint32_t* isect_index_src(const FwdBufs& b, uint32_t v) {
   return b.pack_bits ? b.isect_key + (size_t)b.Icap * v : b.isect_val + (size_t)b.Icap * v;
 }
 __device__ __forceinline__ uint32_t isect_index_mask(const FwdBufs& b) {
   return b.pack_bits ? (1u << b.pack_bits) - 1u : 0xffffffffu;
 }
+inline uint32_t isect_index_mask_host(const FwdBufs& b) { return b.pack_bits ? (1u << b.pack_bits) - 1u : 0xffffffffu; }
 
 struct ViewSet {
   const ViewDesc* views;  // device
@@ -67,8 +68,10 @@ struct ViewSet {
   uint32_t batch;         // Gaussians per shared-memory batch of the rasterizer (0: tuned defaults)
   uint32_t total_tiles;   // sum over views of tiles_x * tiles_y
   uint32_t max_tiles;     // max over views
-  int persistent;         // raster work: 1 persistent CTAs taking cost-ordered items, 0 one CTA per item
+  int persistent;         // kPersist* bits: raster kernels whose CTAs take cost-ordered items persistently
 };
+// Bits of ViewSet::persistent (otherwise one CTA per work item).
+constexpr int kPersistFwd = 1, kPersistBwd = 2;
 
 struct SplatsDev {
   const float* transforms;

@@ -49,8 +49,9 @@ constexpr int kWalkBlocksPerSm = 24;
 // box, never cull).
 // SLOTS (emission only): every box tile of a Gaussian has a slot at its
 // row-major position after the Gaussian's offset (offsets scanned from box
-// sizes, no counting walk); a passing tile writes its packed key there, a
-// failing one the all-ones key, which sorts after every tile.
+// sizes, no counting walk); a passing tile writes its key there (packed, or
+// the tile id with the compact index as value), a failing one the all-ones
+// key, which sorts after every tile.
 template <bool EMIT, bool HIST = false, bool SLOTS = false>
 __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, FwdBufs b, int det) {
   __shared__ WalkWarp s_w[kWalkWarps];
@@ -153,10 +154,11 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
           if (o < cap) {
             if (pass) {
               if (HIST) atomicAdd(&s_th[tx + ty * vd.tiles_x], 1u);
-              keys[o] = ((tx + ty * vd.tiles_x) << b.pack_bits) | S.cid[owner];
+              keys[o] = b.pack_bits ? ((tx + ty * vd.tiles_x) << b.pack_bits) | S.cid[owner] : tx + ty * vd.tiles_x;
             } else {
               keys[o] = 0xffffffffu;
             }
+            if (!b.pack_bits) vals[o] = S.cid[owner];
           }
         }
         continue;
@@ -395,7 +397,7 @@ cudaError_t launch_emit(const ViewSet& vs, FwdBufs& b, const Scratch& s, int det
 cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, int deterministic, bool slots,
                              cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles) return cudaErrorInvalidValue;
-  if (slots && (deterministic || !b.pack_bits)) return cudaErrorInvalidValue;
+  if (slots && deterministic) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(b.tile_hist, 0, sizeof(uint32_t) * b.Tcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   const size_t smem = sizeof(uint32_t) * vs.max_tiles;
@@ -415,12 +417,11 @@ cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch
 }
 
 cudaError_t launch_count_from_isects(FwdBufs& b, uint32_t view, uint32_t n_visible, cudaStream_t st) {
-  if (!b.pack_bits) return cudaErrorInvalidValue;
   uint32_t* count = slice(b.count, b.Vcap, view);
   cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * n_visible, st);
   if (e != cudaSuccess) return e;
-  count_from_isects_kernel<<<1024, 256, 0, st>>>(slice(b.isect_key, b.Icap, view), b.vcount + view * 4 + 1,
-                                                 (1u << b.pack_bits) - 1u, count);
+  count_from_isects_kernel<<<1024, 256, 0, st>>>(isect_index_src(b, view), b.vcount + view * 4 + 1,
+                                                 isect_index_mask_host(b), count);
   return cudaGetLastError();
 }
 

@@ -121,45 +121,36 @@ __global__ void __launch_bounds__(kLT, 5) ssim_fwd_kernel(LossArgs a) {
     for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc[m];
   }
   __syncthreads();
-  // Vertical pass and the SSIM map: each thread slides down one column over
-  // four output rows (the warp's 32 columns of one row group). Rows y and
-  // y + 1 share a paired accumulator, weights (k[r], k[r - 1]) against the
-  // one value loaded from halo row r, and rows y + 2, y + 3 another: 14
-  // loads per plane for 4 outputs. Every output still sums its 11 taps in
-  // tap order (a zero weight adds an exact +0), so the sums equal those of
-  // a per-output loop.
+  // Vertical pass and the SSIM map: a column pair times two rows per thread.
   const float C1 = 1e-4f, C2 = 9e-4f;
   float ssum = 0.f, lsum = 0.f;
   float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
   {
-    constexpr int kRowsPer = LTY / (kLT / LTX);  // 4 output rows per thread
-    static_assert(kRowsPer == 4, "one warp per 4-row group of a 32-column tile");
-    const int ox = threadIdx.x % LTX, oy = kRowsPer * (threadIdx.x / LTX);
-    float2 mo[5][2];  // [plane][pair]: .x row oy + 2 p, .y row oy + 2 p + 1
+    const int ox = 2 * (threadIdx.x % (LTX / 2)), oy = 2 * (threadIdx.x / (LTX / 2));  // 16 x 16 tasks
+    float2 mo[5][2];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
-      float2 pa = f2(0.f), pb = f2(0.f);
+      float2 r0 = f2(0.f), r1 = f2(0.f);
+      float2 prev = *reinterpret_cast<const float2*>(&S.h[m][oy][ox]);
 #pragma unroll
-      for (int r = 0; r < WIN + 3; ++r) {
-        const float2 val = f2(S.h[m][oy + r][ox]);
-        if (r <= WIN)
-          pa = fma2(make_float2(r < WIN ? a.k[r] : 0.f, r >= 1 ? a.k[r - 1] : 0.f), val, pa);
-        if (r >= 2)
-          pb = fma2(make_float2(r - 2 < WIN ? a.k[r - 2] : 0.f, r >= 3 ? a.k[r - 3] : 0.f), val, pb);
+      for (int t = 0; t < WIN; ++t) {
+        const float2 next = *reinterpret_cast<const float2*>(&S.h[m][oy + t + 1][ox]);
+        r0 = fma2(f2(a.k[t]), prev, r0);
+        r1 = fma2(f2(a.k[t]), next, r1);
+        prev = next;
       }
-      mo[m][0] = pa;
-      mo[m][1] = pb;
+      mo[m][0] = r0;
+      mo[m][1] = r1;
     }
 #pragma unroll
-    for (int ry = 0; ry < kRowsPer; ++ry) {
-      {
-        const int cx = 0;
-        const int gx = x0 + ox, gy = y0 + oy + ry;
+    for (int ry = 0; ry < 2; ++ry) {
+#pragma unroll
+      for (int cx = 0; cx < 2; ++cx) {
+        const int gx = x0 + ox + cx, gy = y0 + oy + ry;
         if (gx >= W || gy >= H) continue;
-        const int pr = ry >> 1, hf = ry & 1;
-        const float mx = hf ? mo[0][pr].y : mo[0][pr].x, my = hf ? mo[1][pr].y : mo[1][pr].x;
-        const float exx = hf ? mo[2][pr].y : mo[2][pr].x, eyy = hf ? mo[3][pr].y : mo[3][pr].x;
-        const float exy = hf ? mo[4][pr].y : mo[4][pr].x;
+        const float mx = cx ? mo[0][ry].y : mo[0][ry].x, my = cx ? mo[1][ry].y : mo[1][ry].x;
+        const float exx = cx ? mo[2][ry].y : mo[2][ry].x, eyy = cx ? mo[3][ry].y : mo[3][ry].x;
+        const float exy = cx ? mo[4][ry].y : mo[4][ry].x;
         const float sxx = exx - mx * mx, syy = eyy - my * my, sxy = exy - mx * my;
         const float A = 2.f * mx * my + C1, B = 2.f * sxy + C2;
         const float Cr = mx * mx + my * my + C1, Dr = sxx + syy + C2;
@@ -279,21 +270,41 @@ __global__ void __launch_bounds__(kLT, 5) ssim_bwd_kernel(LossArgs a) {
   // Adjoint of the vertical pass: tile rows, all halo columns (in pairs).
   // When every output row and its taps lie strictly inside the image (no
   // border row, no clamped tap), each tap weighs k[R + d] and no check is
-  // needed; the sums are the same operations in the same order.
+  // needed: a thread then slides down a column pair over four output rows,
+  // adding each loaded halo row into the rows it reaches (14 loads per plane
+  // for 4 rows instead of 44). Every output sums its taps in tap order, as
+  // the per-row loop of border tiles does.
   const bool rows_inside = y0 >= R + 1 && y0 + LTY + R <= H - 1;
-  for (int i = threadIdx.x; i < LTY * (HX / 2); i += blockDim.x) {
+  if (rows_inside) {
+    constexpr int kRows = 4;
+    for (int i = threadIdx.x; i < (LTY / kRows) * (HX / 2); i += blockDim.x) {
+      const int oy = kRows * (i / (HX / 2)), hx = 2 * (i % (HX / 2));
+      float2 acc[3][kRows];
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) acc[m][j] = f2(0.f);
+#pragma unroll
+      for (int r = 0; r < WIN + kRows - 1; ++r) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const float2 val = *reinterpret_cast<const float2*>(&S.g[m][oy + r][hx]);
+#pragma unroll
+          for (int j = 0; j < kRows; ++j)
+            if (r - j >= 0 && r - j < WIN) acc[m][j] = fma2(f2(a.k[r - j]), val, acc[m][j]);
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) *reinterpret_cast<float2*>(&S.v[m][oy + j][hx]) = acc[m][j];
+    }
+  }
+  for (int i = threadIdx.x; !rows_inside && i < LTY * (HX / 2); i += blockDim.x) {
     const int oy = i / (HX / 2), hx = 2 * (i % (HX / 2));
     const int py = y0 + oy;
     float2 acc[3] = {f2(0.f), f2(0.f), f2(0.f)};
-    if (rows_inside) {
-#pragma unroll
-      for (int d = -R; d <= R; ++d) {
-        const float w = a.k[R + d];
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-          acc[m] = fma2(f2(w), *reinterpret_cast<const float2*>(&S.g[m][oy + R + d][hx]), acc[m]);
-      }
-    } else if (py < H) {
+    if (py < H) {
       const bool interior = py > 0 && py < H - 1;
 #pragma unroll
       for (int d = -R; d <= R; ++d) {
@@ -320,13 +331,14 @@ __global__ void __launch_bounds__(kLT, 5) ssim_bwd_kernel(LossArgs a) {
     if (px >= W || py >= H) continue;
     float2 acc[3] = {f2(0.f), f2(0.f), f2(0.f)};
     if (px > 0 && px + 1 < W - 1) {
-      // Both columns interior: the symmetric kernel, paired.
+      // Both columns interior: the symmetric kernel, paired. Each loaded
+      // value serves both columns, weights (k[j], k[j - 1]); a zero weight
+      // adds an exact +0, so each column sums its taps in tap order.
 #pragma unroll
-      for (int d = -R; d <= R; ++d) {
-        const float w = a.k[R + d];
+      for (int j = 0; j <= 2 * R + 1; ++j) {
+        const float2 w = make_float2(j <= 2 * R ? a.k[j] : 0.f, j >= 1 ? a.k[j - 1] : 0.f);
 #pragma unroll
-        for (int m = 0; m < 3; ++m)
-          acc[m] = fma2(f2(w), make_float2(S.v[m][oy][ox + R + d], S.v[m][oy][ox + 1 + R + d]), acc[m]);
+        for (int m = 0; m < 3; ++m) acc[m] = fma2(w, f2(S.v[m][oy][ox + j]), acc[m]);
       }
     } else {
 #pragma unroll

@@ -62,6 +62,7 @@ struct RasterArgs {
   const float* v_rgba;
   int ref_mode;
   int det;
+  int persist;  // this launch runs the persistent schedule
 };
 
 __device__ __forceinline__ uint32_t find_view(const ViewSet& vs, uint32_t item) {
@@ -79,7 +80,7 @@ constexpr uint32_t kNoItem = 0xffffffffu;
 // The leading barrier keeps the previous item's shared state intact until
 // every thread is done with it.
 __device__ __forceinline__ uint32_t next_item(const RasterArgs& a, uint32_t round, uint32_t* s_item) {
-  if (!a.vs.persistent) return round == 0 ? blockIdx.x : kNoItem;
+  if (!a.persist) return round == 0 ? blockIdx.x : kNoItem;
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t slot = atomicAdd(a.b.sched_ticket, 1u);
@@ -881,7 +882,7 @@ inline int pick_batch(uint32_t want, int dflt) {
 template <void (*Kernel)(RasterArgs)>
 cudaError_t launch_items(int threads, const RasterArgs& a, int num_sms, cudaStream_t st) {
   uint32_t grid = a.vs.total_tiles;
-  if (a.vs.persistent) {
+  if (a.persist) {
     static int per_sm = 0;  // one per kernel instantiation
     if (per_sm <= 0) {
       int n = 0;
@@ -939,7 +940,8 @@ cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, fl
   cudaError_t e = cudaMemsetAsync(b.visible_c, 0, b.Vcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.persistent) {
+  a.persist = (vs.persistent & kPersistFwd) != 0;
+  if (a.persist) {
     sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -966,7 +968,8 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     if (e != cudaSuccess) return e;
   }
   if (vs.total_tiles == 0) return cudaSuccess;
-  if (vs.persistent) {
+  a.persist = (vs.persistent & kPersistBwd) != 0;
+  if (a.persist) {
     sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -176,3 +176,29 @@ def test_config3_view0_loss_and_gradients(gsr_ctx_factory, config3):
     # The other views' gradient columns (signed and absolute mean-gradient
     # sums) are zero under a zero upstream gradient.
     assert not gg["stats"][1:, :, 0:5].any()
+
+
+def test_unpacked_slot_layout_above_2_20_gaussians(gsr_ctx_factory):
+    """1,100,000 Gaussians and a 1280x720 view: the compact index (21 bits)
+    and the tile id (12 bits) no longer pack into 32 bits, so the slot
+    layout runs with (tile id, compact index) pairs. Forward bit-exact and
+    gradients within the parity bar, against the FP32 oracle."""
+    import torch
+
+    from rustscan_b200 import host_splats_to_device
+
+    sc = S.config3(n=1_100_000, views=1)
+    cam = sc.cameras[0]
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=1280 * 720, max_isects=24 << 20)
+    splats = host_splats_to_device(sc)
+    _fit(ctx, splats, [cam])
+    _, g = run_gpu_forward(ctx, splats, [cam])
+    o = oracle_forward(sc, cam)
+    assert_forward_parity(g[0], o)
+    np.testing.assert_array_equal(ctx.export(0, "tile_counts"), o.count)
+    up = S.upstream_grad(cam.height, cam.width)
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=False))
+    ob = o.backward(up, mode=0)
+    od = oracle_forward(sc, cam, f64=True).backward(up, mode=0)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"1.1M unpacked {k}")
