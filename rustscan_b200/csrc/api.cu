@@ -435,6 +435,7 @@ gsr_status gsr_sync_status(gsr_ctx* c, void* stream, uint64_t* required) {
     return fail(c, GSR_ERR_TIMEOUT, buf);
   }
   if (h.bad_input) return fail(c, GSR_ERR_INVALID_ARG, "a topology plan row names a source splat out of range");
+  if (h.internal) return fail(c, GSR_ERR_CUDA, "internal check failed: a sort position fell outside its segment");
   if (h.overflow) {
     char buf[128];
     snprintf(buf, sizeof(buf), "intersection capacity %llu exceeded: %llu required",

@@ -19,6 +19,7 @@ struct DevStatus {
   uint32_t timeout_where;  // which wait gave up (kernel id)
   uint32_t bad_input;      // an input index out of range (topology plan)
   unsigned long long required;  // largest intersection count requested
+  uint32_t internal;       // an internal consistency check failed (a sort position outside its segment)
 };
 
 enum : uint32_t { kWaitCompact = 1, kWaitScan = 2, kWaitSort = 3, kWaitSelfTest = 4 };

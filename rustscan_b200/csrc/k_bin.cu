@@ -219,8 +219,7 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
 // tile id's digits, in the sort's histogram layout.
 constexpr int kHistThreads = 1024;
 __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist,
-                                                                         uint32_t dbits, uint32_t sentinel_tile,
-                                                                         int slots) {
+                                                                         uint32_t dbits, int slots) {
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_h[2][256];
   const uint32_t v = blockIdx.x;
@@ -257,11 +256,15 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
   if (slots && threadIdx.x == 0) {
     // Slot layout: the sort covers every slot written (the scanned box
     // sizes, clamped to capacity); the slots of failing tiles hold the
-    // sentinel tile. The view's intersection count becomes the real one.
+    // all-ones key. Its digits are taken as the sort takes them, from bit
+    // pack_bits (0 for pairs) in dbits-wide steps (the top digit of a packed
+    // key can be narrower than dbits); over the sorted bits it exceeds every
+    // tile id, so it sorts last. The view's intersection count becomes the
+    // real one.
     const uint32_t written = b.vcount[v * 4 + 1];
     const uint32_t dm = (1u << dbits) - 1u;
-    atomicAdd(&s_h[0][sentinel_tile & dm], written - all);
-    atomicAdd(&s_h[1][(sentinel_tile >> dbits) & dm], written - all);
+    atomicAdd(&s_h[0][(uint32_t)(0xffffffffull >> b.pack_bits) & dm], written - all);
+    atomicAdd(&s_h[1][(uint32_t)(0xffffffffull >> (b.pack_bits + dbits)) & dm], written - all);
     b.vcount[v * 4 + 3] = written;
     b.vcount[v * 4 + 1] = all;
     b.vcount[v * 4 + 2] = all;
@@ -412,7 +415,7 @@ cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch
                                    cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles || sort_passes(tile_bits) > 2) return cudaErrorInvalidValue;
   tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits),
-                                                                (1u << tile_bits) - 1u, slots ? 1 : 0);
+                                                                slots ? 1 : 0);
   return cudaGetLastError();
 }
 

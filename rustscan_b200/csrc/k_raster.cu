@@ -110,7 +110,17 @@ __global__ void __launch_bounds__(kOrderThreads) sched_order_kernel(ViewSet vs, 
     const uint32_t* r = slice(b.ranges, 2 * b.Tcap, v);
     return r[2 * t + 1] - r[2 * t];
   };
-  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads) atomicAdd(&s_hist[cost_bucket(cost_of(i))], 1u);
+  // Warp-aggregated: the lanes of a warp with the same bucket make one
+  // shared atomic (the costs cluster in a few buckets, where per-item
+  // atomics would serialise).
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lower = (1u << lane) - 1u;
+  for (uint32_t i0 = threadIdx.x - lane; i0 < total; i0 += kOrderThreads) {
+    const uint32_t i = i0 + lane;
+    const uint32_t bk = i < total ? cost_bucket(cost_of(i)) : 64u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, bk);
+    if (bk < 64u && (peers & lower) == 0u) atomicAdd(&s_hist[bk], (uint32_t)__popc(peers));
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t run = 0;
@@ -121,8 +131,16 @@ __global__ void __launch_bounds__(kOrderThreads) sched_order_kernel(ViewSet vs, 
     *b.sched_ticket = 0u;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads)
-    b.sched_order[atomicAdd(&s_start[cost_bucket(cost_of(i))], 1u)] = i;
+  for (uint32_t i0 = threadIdx.x - lane; i0 < total; i0 += kOrderThreads) {
+    const uint32_t i = i0 + lane;
+    const uint32_t bk = i < total ? cost_bucket(cost_of(i)) : 64u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, bk);
+    const uint32_t leader = (uint32_t)__ffs(peers) - 1u;
+    uint32_t base = 0u;
+    if (bk < 64u && lane == leader) base = atomicAdd(&s_start[bk], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, (int)leader);
+    if (bk < 64u) b.sched_order[base + (uint32_t)__popc(peers & lower)] = i;
+  }
 }
 
 // Warp w of a TW-wide tile owns the 8 x (4*PPL) block at (x0, y0); lane l

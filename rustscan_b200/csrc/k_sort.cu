@@ -192,8 +192,14 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
       const uint32_t k = s_keys[j];
       const uint32_t dst = s_gbase[(k >> a.shift) & a.dmask] + j;
-      kout[dst] = k;
-      if (KV) vout[dst] = s_vals[j];
+      // A position outside the segment means the digit histogram did not
+      // describe these keys: it is reported, never written.
+      if (dst < n) {
+        kout[dst] = k;
+        if (KV) vout[dst] = s_vals[j];
+      } else {
+        atomicOr(&a.status->internal, 1u);
+      }
     }
   }
   epoch_end(a.ctl, epoch);

@@ -202,3 +202,27 @@ def test_unpacked_slot_layout_above_2_20_gaussians(gsr_ctx_factory):
     od = oracle_forward(sc, cam, f64=True).backward(up, mode=0)
     for k in ("v_transforms", "v_sh", "v_raw_opacity"):
         assert_grad_parity(gg[k], ob[k], od[k], what=f"1.1M unpacked {k}")
+
+
+@pytest.mark.parametrize("n, size", [(200_000, (640, 480)), (600_000, (1920, 1080)), (30_000, (320, 240))],
+                         ids=["packed-11-tile-bits", "pairs-13-tile-bits", "packed-9-tile-bits"])
+def test_slot_sort_at_exact_capacity(gsr_ctx_factory, n, size):
+    """The slot layout at an intersection capacity equal to the slots
+    written, with an odd number of tile-id bits (the sort's digits do not
+    split the tile id evenly): every sort position stays inside its
+    segment (the sort reports any that would not, instead of writing it)
+    and the forward is bit-exact against the oracle. Packed keys and (tile
+    id, compact index) pairs."""
+    from rustscan_b200 import GsrError, host_splats_to_device
+
+    w, h = size
+    sc = S.config3(n=n, views=1, width=w, height=h, focal=1050.0 * w / 1280.0)
+    cam = sc.cameras[0]
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=w * h, max_isects=1 << 16)
+    splats = host_splats_to_device(sc)
+    with pytest.raises(GsrError) as ei:
+        ctx.render_forward(splats, [cam], check=True)
+    assert ei.value.status == 3
+    ctx.reserve_isects(ei.value.required)
+    _, g = run_gpu_forward(ctx, splats, [cam])  # raises on any status, the sort's range check included
+    assert_forward_parity(g[0], oracle_forward(sc, cam))
