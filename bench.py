@@ -28,8 +28,9 @@ METRIC = "fwd+bwd ms/view (1M Gaussians, 1280x720) batched vs plain; grad rel er
 UNIT = "ms/view"
 WORKLOAD = "batched training step: 1,000,000 Gaussians, SH degree 3, 8 views of 1280x720 per step"
 # ncu smsp__inst_executed.sum of the raster kernels on one 1280x720 view of
-# this workload (6,273,269 intersections), per intersection.
-WARP_INST_PER_ISECT = {"raster_bwd": 205.9e6 / 6273269, "raster_fwd": 152.5e6 / 6273269}
+# this workload (6,273,269 intersections), per intersection
+# (profiles/raster_c3_1view_issue.md).
+WARP_INST_PER_ISECT = {"raster_bwd": 217.03e6 / 6273269, "raster_fwd": 150.76e6 / 6273269}
 
 
 def parse():
