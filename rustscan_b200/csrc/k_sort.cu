@@ -19,6 +19,8 @@
 // tie-break provides (radix_sort.wgsl:21-26). Without values, the keys are
 // sorted alone (the binning packs tile id and compact index into one key
 // when both fit in 32 bits).
+#include <algorithm>
+
 #include "gsr_kernels.h"
 
 namespace gsr {
@@ -233,13 +235,14 @@ struct ScanArgs {
   uint32_t parts_cap;
   LookbackCtl* ctl;
   DevStatus* status;
+  uint32_t seg_base;  // segment of blockIdx.y == 0
 };
 
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(ScanArgs a) {
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_ticket, s_excl;
   const uint32_t epoch = epoch_begin(a.ctl);
-  const uint32_t seg = blockIdx.y;
+  const uint32_t seg = a.seg_base + blockIdx.y;
   const uint32_t n = seg_count(a.counts, a.count_stride, seg, a.n_host, a.cap);
   const uint32_t* in = a.in + (size_t)seg * a.seg_stride;
   const uint32_t* ga = a.gather ? a.gather + (size_t)seg * a.seg_stride : nullptr;
@@ -419,7 +422,17 @@ cudaError_t launch_offsets(const ViewSet& vs, FwdBufs& b, const Scratch& s, cuda
   a.states = s.lb_states;
   a.ctl = s.ctl;
   a.status = s.status;
-  scan_kernel<<<dim3(persistent_blocks(s.num_sms, vs.n_views, 4), vs.n_views), kScanThreads, 0, st>>>(a);
+  // The scan gathers the counts through the depth order, one 4-byte read
+  // per random index. Views are scanned in groups whose count arrays fit in
+  // about a third of L2 together, so each 32-byte sector is fetched from
+  // DRAM once rather than once per element read from it.
+  constexpr uint64_t kGatherBytes = 40ull << 20;
+  const uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(vs.n_views, kGatherBytes / (4 * b.Vcap)));
+  for (uint32_t v0 = 0; v0 < vs.n_views; v0 += per) {
+    const uint32_t nv = std::min(per, vs.n_views - v0);
+    a.seg_base = v0;
+    scan_kernel<<<dim3(persistent_blocks(s.num_sms, nv, 4), nv), kScanThreads, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -136,6 +136,7 @@ def test_config3_forward_all_views(gsr_ctx_factory, config3, batch):
         report(f"config3 view {v} forward (batch {batch})", visible=o.num_visible, intersections=o.num_intersections,
                image_max_abs=float(np.abs(g[v]["image"] - o.image).max()))
         del o
+    ctx.close()
 
 
 def test_config3_view0_loss_and_gradients(gsr_ctx_factory, config3):
@@ -226,3 +227,70 @@ def test_slot_sort_at_exact_capacity(gsr_ctx_factory, n, size):
     ctx.reserve_isects(ei.value.required)
     _, g = run_gpu_forward(ctx, splats, [cam])  # raises on any status, the sort's range check included
     assert_forward_parity(g[0], oracle_forward(sc, cam))
+
+
+# ---- configs 4 and 5 at their stated sizes ---------------------------------------
+
+
+def test_config4_full_size_bf16_fp64_conic(gsr_ctx_factory):
+    """Config 4 as stated: 3,000,000 Gaussians (5% with one log-scale at -9),
+    SH degree 3 in BF16 storage, one 1920x1080 view at fx = fy = 1400, the
+    FP64 conic. Against the oracle in FP64-conic mode fed the stored
+    (BF16-rounded) SH: integer outputs bit-exact, image within 1e-5,
+    gradients within the parity bar."""
+    import torch
+
+    from oracle import oracle as O
+    from rustscan_b200 import host_splats_to_device
+
+    sc = S.config4()
+    cam = sc.cameras[0]
+    sh_r = torch.as_tensor(sc.sh).to(torch.bfloat16).to(torch.float32).numpy()
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=1920 * 1080, max_isects=48 << 20, sh_dtype="bf16",
+                          fp64_conic=True)
+    splats = host_splats_to_device(sc, sh_dtype=torch.bfloat16)
+    _fit(ctx, splats, [cam])
+    _, g = run_gpu_forward(ctx, splats, [cam])
+    o = O.Forward(sc.transforms, sh_r, sc.raw_opacity, 3, cam, fp64_conic=True)
+    assert o.num_intersections > 10_000_000
+    assert_forward_parity(g[0], o)
+    up = S.upstream_grad(cam.height, cam.width)
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=False))
+    ob = o.backward(up, mode=0)
+    od = O.Forward(sc.transforms, sh_r, sc.raw_opacity, 3, cam, f64=True, fp64_conic=True).backward(
+        up.astype(np.float64), mode=0)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"config4 {k}")
+    ctx.close()
+
+
+def test_config5_full_size_views_bit_exact(gsr_ctx_factory):
+    """Config 5 as stated: 2,000,000 Gaussians, 32 views of mixed resolution
+    in one launch per stage, BF16 SH storage. One view of each resolution
+    (and the view with the fewest visible Gaussians) against the oracle fed
+    the stored SH: integer outputs bit-exact, images within 1e-5."""
+    import torch
+
+    from oracle import oracle as O
+    from rustscan_b200 import host_splats_to_device
+
+    sc = S.config5()
+    cams = sc.cameras
+    pmax = max(c.width * c.height for c in cams)
+    sh_r = torch.as_tensor(sc.sh).to(torch.bfloat16).to(torch.float32).numpy()
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=len(cams), max_pixels=pmax, max_isects=24 << 20,
+                          sh_dtype="bf16")
+    splats = host_splats_to_device(sc, sh_dtype=torch.bfloat16)
+    _fit(ctx, splats, cams)
+    _, g = run_gpu_forward(ctx, splats, cams)
+    picks = {}
+    for v, c in enumerate(cams):
+        picks.setdefault((c.width, c.height), v)
+    picks = sorted(set(picks.values()) | {int(np.argmin([int(d["counts"][0]) for d in g]))})
+    for v in picks:
+        o = O.Forward(sc.transforms, sh_r, sc.raw_opacity, 3, cams[v])
+        assert_forward_parity(g[v], o)
+        report(f"config5 view {v} forward ({cams[v].width}x{cams[v].height})", visible=o.num_visible,
+               intersections=o.num_intersections)
+        del o
+    ctx.close()  # large capacities: released now, not at the end of the session
