@@ -6,7 +6,7 @@
 // C2 = 9e-4 and denominators clamped at 1e-8. The reference builds it from
 // ~10 burn ops and differentiates through burn autodiff; here two tiled
 // kernels do the work:
-//  pass 1: per 32x32 output tile and channel, the five blurred moments in
+//  pass 1: per 32x32 output tile and channel, the four blurred moments in
 //          shared memory, the SSIM map, its partial derivatives with respect
 //          to (mu_x, E[x^2], E[xy]) and per-tile partial sums of SSIM and L1;
 //  pass 2: the adjoint of the padded separable blur applied to the three
@@ -41,14 +41,17 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 // Pass 1. Shared memory holds the two input planes (x, y) of the
-// replicate-padded halo, then the five horizontally blurred planes (x, y,
-// x^2, y^2, xy; the products are formed as the row is read). Each thread
+// replicate-padded halo, then the four horizontally blurred planes (x, y,
+// x^2 + y^2, xy; the products are formed as the row is read). SSIM needs
+// E[x^2] and E[y^2] only through their sum (in sigma_x^2 + sigma_y^2), and
+// its derivatives with respect to both are equal, so one blurred plane
+// carries the sum. Each thread
 // blurs two adjacent columns at once with paired FP32 arithmetic, sliding
 // one load per tap along the row (horizontal) or down the column pair
 // (vertical, two output rows per thread).
 struct SsimFwdSmem {
   float p[2][HY][HX];
-  float h[5][HY][LTX];
+  float h[4][HY][LTX];
   float red[2][8];
 };
 
@@ -89,36 +92,35 @@ __global__ void __launch_bounds__(kLT, 5) ssim_fwd_kernel(LossArgs a) {
     }
   }
   __syncthreads();
-  // Horizontal pass: every halo row, output columns in pairs; the five
+  // Horizontal pass: every halo row, output columns in pairs; the four
   // moment values of each input are formed once from x and y.
   for (int i = threadIdx.x; i < HY * (LTX / 2); i += blockDim.x) {
     const int hy = i / (LTX / 2), ox = 2 * (i % (LTX / 2));
     const float* rx = &S.p[0][hy][ox];
     const float* ry = &S.p[1][hy][ox];
-    float2 acc[5];
-    float prev[5];
+    float2 acc[4];
+    float prev[4];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) acc[m] = f2(0.f);
+    for (int m = 0; m < 4; ++m) acc[m] = f2(0.f);
     {
       const float x = rx[0], y = ry[0];
       prev[0] = x;
       prev[1] = y;
-      prev[2] = x * x;
-      prev[3] = y * y;
-      prev[4] = x * y;
+      prev[2] = x * x + y * y;
+      prev[3] = x * y;
     }
 #pragma unroll
     for (int t = 0; t < WIN; ++t) {
       const float x = rx[t + 1], y = ry[t + 1];
-      const float next[5] = {x, y, x * x, y * y, x * y};
+      const float next[4] = {x, y, x * x + y * y, x * y};
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
+      for (int m = 0; m < 4; ++m) {
         acc[m] = fma2(f2(a.k[t]), make_float2(prev[m], next[m]), acc[m]);
         prev[m] = next[m];
       }
     }
 #pragma unroll
-    for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc[m];
+    for (int m = 0; m < 4; ++m) *reinterpret_cast<float2*>(&S.h[m][hy][ox]) = acc[m];
   }
   __syncthreads();
   // Vertical pass and the SSIM map: a column pair times two rows per thread.
@@ -127,9 +129,9 @@ __global__ void __launch_bounds__(kLT, 5) ssim_fwd_kernel(LossArgs a) {
   float* maps = a.maps + ((size_t)v * 3 + ch) * 3 * a.Pcap;
   {
     const int ox = 2 * (threadIdx.x % (LTX / 2)), oy = 2 * (threadIdx.x / (LTX / 2));  // 16 x 16 tasks
-    float2 mo[5][2];
+    float2 mo[4][2];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
+    for (int m = 0; m < 4; ++m) {
       float2 r0 = f2(0.f), r1 = f2(0.f);
       float2 prev = *reinterpret_cast<const float2*>(&S.h[m][oy][ox]);
 #pragma unroll
@@ -149,11 +151,11 @@ __global__ void __launch_bounds__(kLT, 5) ssim_fwd_kernel(LossArgs a) {
         const int gx = x0 + ox + cx, gy = y0 + oy + ry;
         if (gx >= W || gy >= H) continue;
         const float mx = cx ? mo[0][ry].y : mo[0][ry].x, my = cx ? mo[1][ry].y : mo[1][ry].x;
-        const float exx = cx ? mo[2][ry].y : mo[2][ry].x, eyy = cx ? mo[3][ry].y : mo[3][ry].x;
-        const float exy = cx ? mo[4][ry].y : mo[4][ry].x;
-        const float sxx = exx - mx * mx, syy = eyy - my * my, sxy = exy - mx * my;
+        const float ess = cx ? mo[2][ry].y : mo[2][ry].x;  // E[x^2] + E[y^2]
+        const float exy = cx ? mo[3][ry].y : mo[3][ry].x;
+        const float sxy = exy - mx * my;
         const float A = 2.f * mx * my + C1, B = 2.f * sxy + C2;
-        const float Cr = mx * mx + my * my + C1, Dr = sxx + syy + C2;
+        const float Cr = mx * mx + my * my + C1, Dr = ((ess - mx * mx) - my * my) + C2;
         const float Cc = fmaxf(Cr, 1e-8f), Dc = fmaxf(Dr, 1e-8f);
         const float inv = 1.f / (Cc * Dc);
         const float s = (A * B) * inv;

@@ -178,7 +178,15 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     const uint32_t excl = d <= a.dmask ? lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort) : 0u;
     s_dstart[d] = dstart;
     s_gbase[d] = gbase[d] + excl - dstart;
-    __syncthreads();
+    // This partition writes digit d's keys to gbase[d] + excl onwards; a
+    // position past the segment would mean the digit histogram did not
+    // describe these keys. Such a partition writes nothing and is reported
+    // through the status words.
+    const bool outside = d <= a.dmask && sum != 0u && (uint64_t)gbase[d] + excl + sum > n;
+    if (__syncthreads_or(outside)) {
+      if (threadIdx.x == 0) atomicOr(&a.status->internal, 1u);
+      continue;
+    }
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
@@ -194,14 +202,8 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
       const uint32_t k = s_keys[j];
       const uint32_t dst = s_gbase[(k >> a.shift) & a.dmask] + j;
-      // A position outside the segment means the digit histogram did not
-      // describe these keys: it is reported, never written.
-      if (dst < n) {
-        kout[dst] = k;
-        if (KV) vout[dst] = s_vals[j];
-      } else {
-        atomicOr(&a.status->internal, 1u);
-      }
+      kout[dst] = k;
+      if (KV) vout[dst] = s_vals[j];
     }
   }
   epoch_end(a.ctl, epoch);
