@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     // position past the segment would mean the digit histogram did not
     // describe these keys. Such a partition writes nothing and is reported
     // through the status words.
-    const bool outside = d <= a.dmask && sum != 0u && (uint64_t)gbase[d] + excl + sum > n;
+    const bool outside = sum != 0u && s_gbase[d] + dstart + sum > n;  // 32 bits suffice: each term is below 2^30
     if (__syncthreads_or(outside)) {
       if (threadIdx.x == 0) atomicOr(&a.status->internal, 1u);
       continue;
