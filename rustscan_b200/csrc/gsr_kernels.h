@@ -44,9 +44,11 @@ struct FwdBufs {
   float* sgrad_part;       // [I][12] per-intersection partial sums (deterministic mode)
   uint32_t* inv_perm;      // [I] emission index -> sorted position (deterministic mode)
   uint32_t* vcount;        // [4] visible, intersections (clamped), intersections required, pad
-  uint32_t* sched_order;   // [views * Tcap] raster work items in issue order (persistent schedule)
-  uint32_t* sched_work;    // [views * Tcap] per work item: list entries up to the tile's last contributor
-  uint32_t* sched_ticket;  // [1] next slot of sched_order a persistent raster CTA takes
+  uint32_t* sched_order;   // [views * Tcap] persistent forward: work items in issue order
+  uint32_t* sched_lists;   // [33][sched_items_cap] work items by the bit length of their backward cost
+  uint32_t* sched_lcount;  // [33] items in each of those lists (appended by the forward)
+  uint32_t* sched_ticket;  // [1] next ticket a persistent raster CTA takes
+  uint64_t sched_items_cap;
   uint64_t Vcap, Ncap, Icap, Tcap, Pcap;
   uint32_t pack_bits;      // > 0: intersections are packed keys (see isect_key), else (tile, index) pairs
   bool slots;              // slot layout: one key per box tile, sentinel keys last; vcount[3] = keys sorted

@@ -30,15 +30,16 @@
 // order).
 //
 // Work items are the (view, tile) pairs of the launch. With the persistent
-// schedule a single-block kernel first orders the items by decreasing
-// estimated cost (counting sort over the bit length of the cost: the list
-// length for the forward, the entries up to the tile's last contributor for
-// the backward, which the forward records per item), and the raster kernels
-// run as many CTAs as the SMs hold at once, each taking the next item from
-// an atomic ticket. The longest tiles start first, so the launch does not
+// schedule the raster kernels run as many CTAs as the SMs hold at once, each
+// taking the next item from an atomic ticket, in decreasing order of an
+// estimated cost, so the longest tiles start first and the launch does not
 // end in a tail of long tiles on a few SMs; views of different sizes and
-// visible counts share one queue. Otherwise one CTA per item runs in item
-// order.
+// visible counts share one queue. The backward's cost is the number of list
+// entries up to the tile's last contributor: the forward appends each item
+// to the list of its cost's bit length (33 lists), and a backward ticket
+// walks the lists from the longest costs down. A persistent forward orders
+// its items by list length with a single-block counting sort first.
+// Otherwise one CTA per item runs in item order.
 #include <algorithm>
 
 #include "gsr_kernels.h"
@@ -62,7 +63,7 @@ struct RasterArgs {
   const float* v_rgba;
   int ref_mode;
   int det;
-  int persist;  // this launch runs the persistent schedule
+  int persist;  // 0: one CTA per item; 1: persistent, items from sched_order; 2: persistent, items from the cost lists
 };
 
 __device__ __forceinline__ uint32_t find_view(const ViewSet& vs, uint32_t item) {
@@ -74,73 +75,88 @@ __device__ __forceinline__ uint32_t find_view(const ViewSet& vs, uint32_t item) 
 
 constexpr uint32_t kNoItem = 0xffffffffu;
 
+constexpr int kCostLists = 33;  // bit lengths 0..32 of a cost
+
+__device__ __forceinline__ uint32_t cost_bucket(uint32_t cost) { return cost ? 32u - (uint32_t)__clz(cost) : 0u; }
+
+// Per CTA, for the cost lists: each list's length and its first ticket
+// (lists in decreasing cost order). Read once per launch.
+struct CostListView {
+  uint32_t count[kCostLists];
+  uint32_t first[kCostLists];
+};
+__device__ __forceinline__ void load_cost_lists(const RasterArgs& a, CostListView* s) {
+  if (a.persist != 2) return;
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = kCostLists - 1; k >= 0; --k) {
+      const uint32_t n = a.b.sched_lcount[k];
+      s->count[k] = n;
+      s->first[k] = run;
+      run += n;
+    }
+  }
+}
+
 // The next work item of this CTA (block-uniform; kNoItem when done). In
 // the grid schedule a CTA runs item blockIdx.x once; in the persistent one
-// thread 0 takes a ticket and reads the item at that slot of the cost order.
-// The leading barrier keeps the previous item's shared state intact until
-// every thread is done with it.
-__device__ __forceinline__ uint32_t next_item(const RasterArgs& a, uint32_t round, uint32_t* s_item) {
+// thread 0 takes a ticket and reads the item at that place of the cost
+// order. The leading barrier keeps the previous item's shared state intact
+// until every thread is done with it (and publishes load_cost_lists).
+__device__ __forceinline__ uint32_t next_item(const RasterArgs& a, uint32_t round, uint32_t* s_item,
+                                              const CostListView* lists) {
   if (!a.persist) return round == 0 ? blockIdx.x : kNoItem;
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t slot = atomicAdd(a.b.sched_ticket, 1u);
-    *s_item = slot < a.vs.total_tiles ? a.b.sched_order[slot] : kNoItem;
+    uint32_t item = kNoItem;
+    if (slot < a.vs.total_tiles) {
+      if (a.persist == 1) {
+        item = a.b.sched_order[slot];
+      } else {
+        for (int k = kCostLists - 1; k >= 0; --k) {
+          if (slot - lists->first[k] < lists->count[k]) {
+            item = a.b.sched_lists[(size_t)k * a.b.sched_items_cap + (slot - lists->first[k])];
+            break;
+          }
+        }
+      }
+    }
+    *s_item = item;
   }
   __syncthreads();
   return *s_item;
 }
 
-__device__ __forceinline__ uint32_t cost_bucket(uint32_t cost) { return cost ? 32u - (uint32_t)__clz(cost) : 0u; }
-
-// One block: the work items of the launch in decreasing order of cost
-// bucket (bit length of the cost; order within a bucket is arbitrary), and
-// the ticket reset. BWD selects the backward's cost (recorded by the
-// forward), else the list length.
+// One block: the work items of a persistent forward in decreasing order of
+// cost bucket (bit length of the list length; order within a bucket is
+// arbitrary), and the ticket reset.
 constexpr int kOrderThreads = 1024;
-__global__ void __launch_bounds__(kOrderThreads) sched_order_kernel(ViewSet vs, FwdBufs b, int bwd) {
-  __shared__ uint32_t s_hist[33];
-  __shared__ uint32_t s_start[33];
-  if (threadIdx.x < 33) s_hist[threadIdx.x] = 0;
+__global__ void __launch_bounds__(kOrderThreads) sched_order_kernel(ViewSet vs, FwdBufs b) {
+  __shared__ uint32_t s_hist[kCostLists];
+  __shared__ uint32_t s_start[kCostLists];
+  if (threadIdx.x < kCostLists) s_hist[threadIdx.x] = 0;
   __syncthreads();
   const uint32_t total = vs.total_tiles;
   auto cost_of = [&](uint32_t item) -> uint32_t {
-    if (bwd) return b.sched_work[item];
     const uint32_t v = find_view(vs, item);
     const uint32_t t = item - vs.views[v].tile_base;
     const uint32_t* r = slice(b.ranges, 2 * b.Tcap, v);
     return r[2 * t + 1] - r[2 * t];
   };
-  // Warp-aggregated: the lanes of a warp with the same bucket make one
-  // shared atomic (the costs cluster in a few buckets, where per-item
-  // atomics would serialise).
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t lower = (1u << lane) - 1u;
-  for (uint32_t i0 = threadIdx.x - lane; i0 < total; i0 += kOrderThreads) {
-    const uint32_t i = i0 + lane;
-    const uint32_t bk = i < total ? cost_bucket(cost_of(i)) : 64u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, bk);
-    if (bk < 64u && (peers & lower) == 0u) atomicAdd(&s_hist[bk], (uint32_t)__popc(peers));
-  }
+  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads) atomicAdd(&s_hist[cost_bucket(cost_of(i))], 1u);
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t run = 0;
-    for (int k = 32; k >= 0; --k) {
+    for (int k = kCostLists - 1; k >= 0; --k) {
       s_start[k] = run;
       run += s_hist[k];
     }
     *b.sched_ticket = 0u;
   }
   __syncthreads();
-  for (uint32_t i0 = threadIdx.x - lane; i0 < total; i0 += kOrderThreads) {
-    const uint32_t i = i0 + lane;
-    const uint32_t bk = i < total ? cost_bucket(cost_of(i)) : 64u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, bk);
-    const uint32_t leader = (uint32_t)__ffs(peers) - 1u;
-    uint32_t base = 0u;
-    if (bk < 64u && lane == leader) base = atomicAdd(&s_start[bk], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, (int)leader);
-    if (bk < 64u) b.sched_order[base + (uint32_t)__popc(peers & lower)] = i;
-  }
+  for (uint32_t i = threadIdx.x; i < total; i += kOrderThreads)
+    b.sched_order[atomicAdd(&s_start[cost_bucket(cost_of(i))], 1u)] = i;
 }
 
 // Warp w of a TW-wide tile owns the 8 x (4*PPL) block at (x0, y0); lane l
@@ -272,9 +288,11 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   __shared__ uint16_t s_list[NW][BATCH];
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_work;
+  __shared__ CostListView s_lists;
   if (threadIdx.x == 0) s_work = 0u;
+  load_cost_lists(a, &s_lists);
   for (uint32_t round = 0;; ++round) {
-    const uint32_t item = next_item(a, round, &s_item);
+    const uint32_t item = next_item(a, round, &s_item, &s_lists);
     if (item == kNoItem) break;
     const uint32_t v = find_view(a.vs, item);
     const ViewDesc& vd = a.vs.views[v];
@@ -445,7 +463,9 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
     if (lane == 0 && ml) atomicMax(&s_work, ml);
     __syncthreads();
     if (threadIdx.x == 0) {
-      a.b.sched_work[item] = s_work > s0 ? s_work - s0 : 0u;
+      const uint32_t cost = s_work > s0 ? s_work - s0 : 0u;
+      const uint32_t k = cost_bucket(cost);
+      a.b.sched_lists[(size_t)k * a.b.sched_items_cap + atomicAdd(a.b.sched_lcount + k, 1u)] = item;
       s_work = 0u;
     }
   }
@@ -682,8 +702,10 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   __shared__ float4 s_part[NW][BATCH][3];      // written by the warps whose bit is set
   __shared__ uint32_t s_max;
   __shared__ uint32_t s_item;
+  __shared__ CostListView s_lists;
+  load_cost_lists(a, &s_lists);
   for (uint32_t round = 0;; ++round) {
-    const uint32_t item = next_item(a, round, &s_item);
+    const uint32_t item = next_item(a, round, &s_item, &s_lists);
     if (item == kNoItem) break;
     const uint32_t v = find_view(a.vs, item);
     const ViewDesc& vd = a.vs.views[v];
@@ -958,9 +980,12 @@ cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, fl
   cudaError_t e = cudaMemsetAsync(b.visible_c, 0, b.Vcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   if (vs.total_tiles == 0) return cudaSuccess;
-  a.persist = (vs.persistent & kPersistFwd) != 0;
+  // The forward appends every item to the cost list of its backward cost.
+  e = cudaMemsetAsync(b.sched_lcount, 0, sizeof(uint32_t) * kCostLists, st);
+  if (e != cudaSuccess) return e;
+  a.persist = (vs.persistent & kPersistFwd) != 0 ? 1 : 0;
   if (a.persist) {
-    sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 0);
+    sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -986,10 +1011,9 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     if (e != cudaSuccess) return e;
   }
   if (vs.total_tiles == 0) return cudaSuccess;
-  a.persist = (vs.persistent & kPersistBwd) != 0;
+  a.persist = (vs.persistent & kPersistBwd) != 0 ? 2 : 0;
   if (a.persist) {
-    sched_order_kernel<<<1, kOrderThreads, 0, st>>>(vs, b, 1);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(b.sched_ticket, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
   }
   if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.batch, s.num_sms, st);
