@@ -108,7 +108,10 @@ cudaError_t launch_project(const SplatsDev& sp, const ViewSet& vs, float cov_blu
 // (or n_host when counts is null). vals_in == nullptr means values 0..n-1;
 // vals_out == nullptr sorts the keys alone. The digits are `bits` bits
 // from bit shift0 up. The result lands in keys_out/vals_out; tmp buffers
-// are clobbered.
+// are clobbered. With counts_dropped (histograms from the caller, digits
+// below 8 bits), keys equal to 0xffffffff are dropped in the first pass:
+// the histograms must not count them, and counts_dropped[i * count_stride]
+// gives segment i's count without them (the sorted output's length).
 // Radix passes and digit width for a sort over `bits` key bits.
 inline int sort_passes(int bits) {
   const int p = (bits + 7) / 8;
@@ -123,7 +126,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
                              uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
                              uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st,
-                             bool hist_ready = false, uint32_t shift0 = 0);
+                             bool hist_ready = false, uint32_t shift0 = 0, const uint32_t* counts_dropped = nullptr);
 
 // Bounded-wait self-test: a look-back whose predecessor never publishes
 // (look-back states 0 and 1 are overwritten); gives up after max_polls.
@@ -157,6 +160,7 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
 // Tile ranges and the tile sort's digit histograms (digits of
 // sort_digit_bits(bits_for(max tiles)) bits) from emission's tile counts.
 cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, bool slots,
+                                   bool drop_sentinels,
                                    cudaStream_t st);
 // Packed mode only: the passing-tile counts of a view's compact indices,
 // recounted from its sorted intersections into b.count.

@@ -256,15 +256,19 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
   if (slots && threadIdx.x == 0) {
     // Slot layout: the sort covers every slot written (the scanned box
     // sizes, clamped to capacity); the slots of failing tiles hold the
-    // all-ones key. Its digits are taken as the sort takes them, from bit
-    // pack_bits (0 for pairs) in dbits-wide steps (the top digit of a packed
-    // key can be narrower than dbits); over the sorted bits it exceeds every
-    // tile id, so it sorts last. The view's intersection count becomes the
-    // real one.
+    // all-ones key. Either the sort drops those in its first pass (slots ==
+    // 2, digits below 8 bits) and the histograms count the real keys only,
+    // or they are sorted along (slots == 1): their digits are then counted
+    // as the sort takes them, from bit pack_bits (0 for pairs) in
+    // dbits-wide steps (the top digit of a packed key can be narrower than
+    // dbits); over the sorted bits the key exceeds every tile id, so it
+    // sorts last. The view's intersection count becomes the real one.
     const uint32_t written = b.vcount[v * 4 + 1];
     const uint32_t dm = (1u << dbits) - 1u;
-    atomicAdd(&s_h[0][(uint32_t)(0xffffffffull >> b.pack_bits) & dm], written - all);
-    atomicAdd(&s_h[1][(uint32_t)(0xffffffffull >> (b.pack_bits + dbits)) & dm], written - all);
+    if (slots == 1) {
+      atomicAdd(&s_h[0][(uint32_t)(0xffffffffull >> b.pack_bits) & dm], written - all);
+      atomicAdd(&s_h[1][(uint32_t)(0xffffffffull >> (b.pack_bits + dbits)) & dm], written - all);
+    }  // slots == 2: the sort drops the sentinels in its first pass
     b.vcount[v * 4 + 3] = written;
     b.vcount[v * 4 + 1] = all;
     b.vcount[v * 4 + 2] = all;
@@ -412,10 +416,10 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
 }
 
 cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, bool slots,
-                                   cudaStream_t st) {
+                                   bool drop_sentinels, cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles || sort_passes(tile_bits) > 2) return cudaErrorInvalidValue;
   tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits),
-                                                                slots ? 1 : 0);
+                                                                slots ? (drop_sentinels ? 2 : 1) : 0);
   return cudaGetLastError();
 }
 

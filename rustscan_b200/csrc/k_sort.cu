@@ -83,6 +83,7 @@ struct SortPassArgs {
   uint32_t dmask;  // digit mask: (1 << digit bits) - 1, at most 255
   uint32_t pass;
   const uint32_t* base;  // [seg][4][256]
+  uint32_t drop;         // 1: keys equal to 0xffffffff take digit dmask + 1 and are not written (dmask < 255)
   unsigned long long* states;
   uint32_t parts_cap;
   LookbackCtl* ctl;
@@ -99,9 +100,12 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
   __shared__ uint32_t s_gbase[256];
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_ticket;
+  __shared__ uint32_t s_dropped;
   const uint32_t epoch = epoch_begin(a.ctl);
   const unsigned long long tag = (unsigned long long)(epoch & 0x3fffffffu) << 34;
   const int dbits = __popc(a.dmask);
+  const int rbits = dbits + (a.drop ? 1 : 0);  // digit bits ranked (the dropped keys' digit is dmask + 1)
+  const uint32_t kDropDigit = a.dmask + 1u;
   const uint32_t seg = blockIdx.y;
   const uint32_t n = seg_count(a.counts, a.count_stride, seg, a.n_host, a.cap);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -134,12 +138,12 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
       uint32_t d, peers;
       if (KV) {
         // Near-random digits (depth keys): one ballot per digit bit.
-        d = (key[i] >> a.shift) & a.dmask;
+        d = (a.drop && key[i] == 0xffffffffu) ? kDropDigit : (key[i] >> a.shift) & a.dmask;
         const uint32_t okm = __ballot_sync(0xffffffffu, ok);  // every lane, also past the end
         peers = ok ? okm : (1u << lane);
 #pragma unroll
         for (int bit = 0; bit < 8; ++bit) {
-          if (bit < dbits) {
+          if (bit < rbits) {
             const bool set = (d >> bit) & 1u;
             const uint32_t bb = __ballot_sync(0xffffffffu, set);
             peers &= set ? bb : ~bb;
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
       } else {
         // Clustered digits (tile ids of neighbouring boxes): few distinct
         // values per warp, where match_any is cheaper.
-        d = ok ? ((key[i] >> a.shift) & a.dmask) : (256u + lane);
+        d = ok ? ((a.drop && key[i] == 0xffffffffu) ? kDropDigit : ((key[i] >> a.shift) & a.dmask)) : (256u + lane);
         peers = __match_any_sync(0xffffffffu, d);
       }
       const uint32_t below = peers & lt_mask;
@@ -178,11 +182,14 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     const uint32_t excl = d <= a.dmask ? lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort) : 0u;
     s_dstart[d] = dstart;
     s_gbase[d] = gbase[d] + excl - dstart;
+    // The dropped keys are placed last in the block and never written (one
+    // thread sets the count: the drop digit's, or thread 0 when nothing drops).
+    if (d == (a.drop ? kDropDigit : 0u)) s_dropped = a.drop ? sum : 0u;
     // This partition writes digit d's keys to gbase[d] + excl onwards; a
     // position past the segment would mean the digit histogram did not
     // describe these keys. Such a partition writes nothing and is reported
     // through the status words.
-    const bool outside = sum != 0u && s_gbase[d] + dstart + sum > n;  // 32 bits suffice: each term is below 2^30
+    const bool outside = d <= a.dmask && sum != 0u && s_gbase[d] + dstart + sum > n;  // each term is below 2^30
     if (__syncthreads_or(outside)) {
       if (threadIdx.x == 0) atomicOr(&a.status->internal, 1u);
       continue;
@@ -191,14 +198,14 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     for (int i = 0; i < kSortItems; ++i) {
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       if (idx < n) {
-        const uint32_t dd = (key[i] >> a.shift) & a.dmask;
+        const uint32_t dd = (a.drop && key[i] == 0xffffffffu) ? kDropDigit : (key[i] >> a.shift) & a.dmask;
         const uint32_t pos = s_dstart[dd] + s_whist[warp][dd] + lrank[i];
         s_keys[pos] = key[i];
         if (KV) s_vals[pos] = val[i];
       }
     }
     __syncthreads();
-    const uint32_t nvalid = min((uint32_t)kSortTile, n - tile0);
+    const uint32_t nvalid = min((uint32_t)kSortTile, n - tile0) - s_dropped;
     for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
       const uint32_t k = s_keys[j];
       const uint32_t dst = s_gbase[(k >> a.shift) & a.dmask] + j;
@@ -309,12 +316,16 @@ int persistent_blocks(int num_sms, uint32_t segments, int per_sm) {
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride, uint32_t segments,
                              const uint32_t* counts, uint32_t count_stride, uint32_t n_host, uint64_t cap_per_segment,
-                             int bits, const Scratch& s, cudaStream_t st, bool hist_ready, uint32_t shift0) {
+                             int bits, const Scratch& s, cudaStream_t st, bool hist_ready, uint32_t shift0,
+                             const uint32_t* counts_dropped) {
   if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
   if (shift0 >= 32 || (keys_in == nullptr)) return cudaErrorInvalidValue;
   const bool kv = vals_out != nullptr;
   const int dbits = sort_digit_bits(bits);
   const int passes = sort_passes(bits);
+  // Dropping the all-ones keys in the first pass needs a spare digit value.
+  const bool drop = counts_dropped != nullptr;
+  if (drop && (dbits >= 8 || !hist_ready)) return cudaErrorInvalidValue;
   const uint32_t parts_cap = (uint32_t)((cap_per_segment + kSortTile - 1) / kSortTile);
   if ((uint64_t)parts_cap * 256 * segments > s.lb_states_words) return cudaErrorInvalidValue;
   if (!hist_ready) {
@@ -338,8 +349,9 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.keys_out = ko;
     a.vals_out = vo;
     a.seg_stride = seg_stride;
-    a.counts = counts;
+    a.counts = (drop && p > 0) ? counts_dropped : counts;
     a.count_stride = count_stride;
+    a.drop = (drop && p == 0) ? 1u : 0u;
     a.n_host = n_host;
     a.cap = cap_per_segment;
     a.shift = shift0 + dbits * p;
