@@ -2,15 +2,15 @@
 that file: `name.wgsl:N`, `name.wgsl:A-B` (and comma lists of those) for the
 shaders, and the same for Rust sources cited by a path whose last components
 identify one file of the reference (`engine/trainer.rs:179-191`). Runs when
-the RustScan checkout is at hand (RUSTSCAN_REFERENCE, default
-/root/reference) and skips otherwise."""
+the RustScan checkout is at hand (the directory RUSTSCAN_REFERENCE names, or
+a `reference` directory beside this repository) and skips otherwise."""
 import os
 import re
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("RUSTSCAN_REFERENCE", "/root/reference")
+REF = os.environ.get("RUSTSCAN_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 # Files written by the build's reviewers and surveyors, not by this repository.
 SKIP_FILES = {"VERDICT.md", "SURVEY.md", "ADVICE.md", "BASELINE.md"}
 CITE = re.compile(r"((?:[A-Za-z0-9_]+/)*[A-Za-z0-9_]+\.(?:wgsl|rs)):(\d+(?:-\d+)?(?:,\s?\d+(?:-\d+)?)*)")
