@@ -189,8 +189,10 @@ gsr_status allocate(gsr_ctx* c) {
   if (cudaMemset(c->s.lb_states, 0, sizeof(unsigned long long) * c->states_words) != cudaSuccess ||
       cudaMemset(c->s.ctl, 0, sizeof(LookbackCtl)) != cudaSuccess ||
       cudaMemset(c->s.status, 0, sizeof(DevStatus)) != cudaSuccess ||
-      cudaMemset(b.vcount, 0, sizeof(uint32_t) * 4 * nv) != cudaSuccess)
+      cudaMemset(b.vcount, 0, sizeof(uint32_t) * 4 * nv) != cudaSuccess ||
+      cudaMemset(b.sched_lcount, 0, sizeof(uint32_t) * 33) != cudaSuccess)
     return cuda_fail(c, cudaGetLastError(), "cudaMemset");
+  raster_warm_up(cfg.tile_w, cfg.tile_h, cfg.batch, c->num_sms);
   return GSR_OK;
 }
 

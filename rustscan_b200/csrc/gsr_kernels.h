@@ -172,6 +172,9 @@ cudaError_t launch_unpack_isects(const FwdBufs& b, uint32_t view, uint32_t n, ui
 cudaError_t launch_remap(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 cudaError_t launch_ranges(const ViewSet& vs, FwdBufs& b, const Scratch& s, cudaStream_t st);
 
+// Looks up the residency of the raster kernels of a tile shape and batch
+// (persistent schedule) outside any stream capture; enqueues nothing.
+void raster_warm_up(uint32_t tile_w, uint32_t tile_h, uint32_t batch, int num_sms);
 cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, float* out_rgba, const Scratch& s,
                               cudaStream_t st);
 cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, const float* v_rgba, int ref_mode,

@@ -919,21 +919,28 @@ inline int pick_batch(uint32_t want, int dflt) {
 // Launches kernel over the launch's work items: one CTA per item (grid
 // schedule), or as many CTAs as the SMs hold at once (persistent schedule;
 // the residency of each instantiation is looked up once).
+// Resident CTAs per SM of a raster kernel instantiation, looked up once
+// (context creation warms it up, so that a first launch inside a stream
+// capture needs no lookup).
+template <void (*Kernel)(RasterArgs)> int resident_per_sm(int threads) {
+  static int per_sm = 0;  // one per kernel instantiation
+  if (per_sm <= 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, Kernel, threads, 0) != cudaSuccess || n < 1) {
+      (void)cudaGetLastError();
+      n = 1;
+    }
+    per_sm = n;
+  }
+  return per_sm;
+}
+
 template <void (*Kernel)(RasterArgs)>
 cudaError_t launch_items(int threads, const RasterArgs& a, int num_sms, cudaStream_t st) {
   uint32_t grid = a.vs.total_tiles;
-  if (a.persist) {
-    static int per_sm = 0;  // one per kernel instantiation
-    if (per_sm <= 0) {
-      int n = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, Kernel, threads, 0) != cudaSuccess || n < 1) {
-        (void)cudaGetLastError();
-        n = 1;
-      }
-      per_sm = n;
-    }
-    grid = std::min<uint32_t>(grid, (uint32_t)per_sm * (uint32_t)std::max(num_sms, 1));
-  }
+  if (a.persist)
+    grid = std::min<uint32_t>(grid, (uint32_t)resident_per_sm<Kernel>(threads) * (uint32_t)std::max(num_sms, 1));
+  if (grid == 0) return cudaSuccess;  // a warm-up call (no items)
   Kernel<<<grid, threads, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -967,6 +974,25 @@ cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, c
 }
 
 }  // namespace
+
+void raster_warm_up(uint32_t tile_w, uint32_t tile_h, uint32_t batch, int num_sms) {
+  RasterArgs a{};
+  a.persist = 1;  // total_tiles 0: the launchers only look up the residency
+  a.vs.batch = batch;
+  for (int ref = 0; ref < 2; ++ref) {
+    a.ref_mode = ref;
+    if (tile_w == 16 && tile_h == 16) {
+      (void)launch_fwd_shape<16, 16, kFwdPPL>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<16, 16, kBwdPPL16>(a, batch, num_sms, nullptr);
+    } else if (tile_w == 8 && tile_h == 8) {
+      (void)launch_fwd_shape<8, 8, kFwdPPL>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<8, 8, 2>(a, batch, num_sms, nullptr);
+    } else if (tile_w == 32 && tile_h == 8) {
+      (void)launch_fwd_shape<32, 8, kFwdPPL>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<32, 8, 2>(a, batch, num_sms, nullptr);
+    }
+  }
+}
 
 cudaError_t launch_raster_fwd(const ViewSet& vs, FwdBufs& b, const float* bg, float* out_rgba, const Scratch& s,
                               cudaStream_t st) {
