@@ -32,8 +32,6 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kWarpKeys = kSortItems * 32;  // 512 keys per warp
-constexpr int kSkewed = 256 + 256 / 32;     // 256 digits, one pad word per 32
-__device__ __forceinline__ uint32_t dsk(uint32_t d) { return d + (d >> 5); }
 
 __device__ __forceinline__ uint32_t seg_count(const uint32_t* counts, uint32_t stride, uint32_t seg, uint32_t n_host,
                                               uint64_t cap) {
@@ -97,11 +95,9 @@ template <bool KV>
 __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(SortPassArgs a) {
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[KV ? kSortTile : 1];
-  // Digit-indexed arrays are skewed by one word per 32 digits (dsk), so that
-  // digits d and d + 32, which lanes look up at once, sit in different banks.
-  __shared__ uint32_t s_whist[kSortWarps][kSkewed];
-  __shared__ uint32_t s_dstart[kSkewed];
-  __shared__ uint32_t s_gbase[kSkewed];
+  __shared__ uint32_t s_whist[kSortWarps][256];
+  __shared__ uint32_t s_dstart[256];
+  __shared__ uint32_t s_gbase[256];
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_ticket;
   __shared__ uint32_t s_dropped;
@@ -132,7 +128,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
       key[i] = ok ? kin[idx] : 0xffffffffu;
       val[i] = (KV && ok) ? (vin ? vin[idx] : idx) : 0u;
     }
-    for (int j = lane; j < kSkewed; j += 32) s_whist[warp][j] = 0;
+    for (int j = lane; j < 256; j += 32) s_whist[warp][j] = 0;
     __syncwarp();
     // Stable rank within the warp: rounds in order, lanes in order.
 #pragma unroll
@@ -161,9 +157,9 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
       }
       const uint32_t below = peers & lt_mask;
       uint32_t b = 0;
-      if (ok) b = s_whist[warp][dsk(d)];
+      if (ok) b = s_whist[warp][d];
       __syncwarp();
-      if (ok && below == 0) s_whist[warp][dsk(d)] = b + __popc(peers);
+      if (ok && below == 0) s_whist[warp][d] = b + __popc(peers);
       __syncwarp();
       lrank[i] = b + __popc(below);
     }
@@ -173,8 +169,8 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     uint32_t sum = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t t = s_whist[w][dsk(d)];
-      s_whist[w][dsk(d)] = sum;
+      const uint32_t t = s_whist[w][d];
+      s_whist[w][d] = sum;
       sum += t;
     }
     // The digit counts are published before the block scan, so that later
@@ -184,8 +180,8 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     uint32_t tot;
     const uint32_t dstart = block_exclusive_scan(sum, s_scan, &tot);
     const uint32_t excl = d <= a.dmask ? lookback(states + d, 256, part, sum, epoch, a.status, kWaitSort) : 0u;
-    s_dstart[dsk(d)] = dstart;
-    s_gbase[dsk(d)] = gbase[d] + excl - dstart;
+    s_dstart[d] = dstart;
+    s_gbase[d] = gbase[d] + excl - dstart;
     // The dropped keys are placed last in the block and never written (one
     // thread sets the count: the drop digit's, or thread 0 when nothing drops).
     if (d == (a.drop ? kDropDigit : 0u)) s_dropped = a.drop ? sum : 0u;
@@ -193,7 +189,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     // position past the segment would mean the digit histogram did not
     // describe these keys. Such a partition writes nothing and is reported
     // through the status words.
-    const bool outside = d <= a.dmask && sum != 0u && s_gbase[dsk(d)] + dstart + sum > n;  // each term is below 2^30
+    const bool outside = d <= a.dmask && sum != 0u && s_gbase[d] + dstart + sum > n;  // each term is below 2^30
     if (__syncthreads_or(outside)) {
       if (threadIdx.x == 0) atomicOr(&a.status->internal, 1u);
       continue;
@@ -203,7 +199,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
       const uint32_t idx = tile0 + warp * kWarpKeys + i * 32 + lane;
       if (idx < n) {
         const uint32_t dd = (a.drop && key[i] == 0xffffffffu) ? kDropDigit : (key[i] >> a.shift) & a.dmask;
-        const uint32_t pos = s_dstart[dsk(dd)] + s_whist[warp][dsk(dd)] + lrank[i];
+        const uint32_t pos = s_dstart[dd] + s_whist[warp][dd] + lrank[i];
         s_keys[pos] = key[i];
         if (KV) s_vals[pos] = val[i];
       }
@@ -212,7 +208,7 @@ __global__ void __launch_bounds__(kSortThreads, KV ? 2 : 4) sort_pass_kernel(Sor
     const uint32_t nvalid = min((uint32_t)kSortTile, n - tile0) - s_dropped;
     for (uint32_t j = threadIdx.x; j < nvalid; j += kSortThreads) {
       const uint32_t k = s_keys[j];
-      const uint32_t dst = s_gbase[dsk((k >> a.shift) & a.dmask)] + j;
+      const uint32_t dst = s_gbase[(k >> a.shift) & a.dmask] + j;
       kout[dst] = k;
       if (KV) vout[dst] = s_vals[j];
     }
