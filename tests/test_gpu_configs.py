@@ -294,3 +294,32 @@ def test_config5_full_size_views_bit_exact(gsr_ctx_factory):
                intersections=o.num_intersections)
         del o
     ctx.close()  # large capacities: released now, not at the end of the session
+
+
+@pytest.mark.parametrize("size, tile", [((2560, 1440), (16, 16)), ((1920, 1080), (8, 8))])
+def test_more_tiles_than_emission_histograms_cover(gsr_ctx_factory, size, tile):
+    """Views with more than 8,192 tiles (14,400 and 32,400 here): emission
+    no longer counts intersections per tile, so the binning runs its
+    counting walk, ranked emission, a histogram pass in the sort and the
+    ranges kernel. Forward bit-exact and gradients within the parity bar."""
+    import torch
+
+    from rustscan_b200 import host_splats_to_device
+
+    w, h = size
+    sc = S.config3(n=100_000, views=1, width=w, height=h, focal=1050.0 * w / 1280.0)
+    cam = sc.cameras[0]
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=w * h, max_isects=8 << 20, tile=tile)
+    splats = host_splats_to_device(sc)
+    _fit(ctx, splats, [cam])
+    _, g = run_gpu_forward(ctx, splats, [cam])
+    o = oracle_forward(sc, cam, tile=tile)
+    assert o.tiles_x * o.tiles_y > 8192
+    assert_forward_parity(g[0], o)
+    up = S.upstream_grad(cam.height, cam.width)
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=False))
+    ob = o.backward(up, mode=0)
+    od = oracle_forward(sc, cam, tile=tile, f64=True).backward(up, mode=0)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"{w}x{h} {tile} {k}")
+    ctx.close()
