@@ -522,8 +522,9 @@ __device__ __forceinline__ float warp_reduce_scatter12(float (&x)[12], int lane)
 // Per-pair state of the reverse walk (pixel q = 2k + h is half h of pair k).
 struct BwdPair {
   uint32_t last0, last1;
-  float2 T, K;          // transmittance, background term
-  float2 SV;            // dot(colour accumulated behind the current Gaussian, upstream colour gradient)
+  float2 T;             // transmittance
+  float2 SK;            // the background term plus dot(colour accumulated behind the current Gaussian,
+                        // upstream colour gradient)
   float2 vr, vg, vb;    // upstream colour gradient
 };
 
@@ -547,8 +548,7 @@ __device__ __forceinline__ void load_bwd_pair(const RasterArgs& a, const ViewDes
   p.last0 = last[0];
   p.last1 = last[1];
   p.T = make_float2(T[0], T[1]);
-  p.K = make_float2(K[0], K[1]);
-  p.SV = f2(0.f);
+  p.SK = make_float2(K[0], K[1]);
   p.vr = make_float2(g[0][0], g[1][0]);
   p.vg = make_float2(g[0][1], g[1][1]);
   p.vb = make_float2(g[0][2], g[1][2]);
@@ -562,16 +562,20 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // A lane's sums over its pixels for the current Gaussian. With dx shared
 // by the lane's column and vs the gradient with respect to sigma at each
-// pixel, the mean and conic gradient sums factor through three moments:
-//   sum vs (a dx + b dy) = a dx M0 + b M1,   sum vs dx^2 / 2 = dx^2 / 2 M0,
-//   sum vs dx dy = dx M1,                    sum vs dy^2 / 2 = M2 / 2,
-// with M0 = sum vs, M1 = sum vs dy, M2 = sum vs dy^2. The absolute
-// mean-gradient sums (densification statistics) stay per pixel.
+// pixel, the mean and conic gradient sums factor through three moments,
+// M0 = sum vs, M1 = sum vs dy, M2 = sum vs dy^2:
+//   sum vs (a dx + b dy) = a S1 + b S2,   sum vs (b dx + c dy) = b S1 + c S2,
+//   sum vs dx^2 / 2 = S3 / 2,   sum vs dx dy = S4,   sum vs dy^2 / 2 = S5 / 2,
+// with S1 = dx M0, S2 = M1, S3 = dx^2 M0, S4 = dx M1 and S5 = M2 per lane.
+// The S sums are what the warp reduces; the conic combination runs once per
+// tile, on the CTA's totals. Where the pixel's alpha is not clamped, alpha =
+// opacity * G, so the opacity-path gradient sum va * G over those pixels is
+// -(sum vs) / opacity: M0 serves for both. The absolute mean-gradient sums
+// (densification statistics) stay per pixel.
 struct BwdAcc {
   float2 m0, m1, m2;
   float2 cr, cg, cb;  // colour gradients
-  float2 op;          // opacity-path gradient
-  float ax, ay;       // sums of |d/dx| and |d/dy| of the per-pixel mean gradients
+  float2 ax, ay;      // sums of |d/dx| and |d/dy| of the per-pixel mean gradients
   uint32_t n;         // contributing pixels
 };
 
@@ -621,32 +625,34 @@ __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, floa
   float2 ra = make_float2(rcp_approx(om.x), rcp_approx(om.y));
   ra = fma2(ra, fma2(neg2(om), ra, f2(1.f)), ra);
 #endif
-  ra = make_float2(c0 ? ra.x : 1.f, c1 ? ra.y : 1.f);
+  // A pixel that does not take the Gaussian has om = 1 exactly, so ra = 1
+  // exactly (the refined reciprocal of 1 is 1) and its state is unchanged.
   const float2 Ti = mul2(p.T, ra);
   const float2 vis = mul2(am, Ti);
   // The colour behind only enters through its dot product with the
   // upstream gradient, which accumulates directly: sum vis_i * dot(c_i, v).
-  const float2 va = fma2(Ti, cpv, neg2(mul2(add2(p.SV, p.K), ra)));
-  p.SV = fma2(vis, cpv, p.SV);
+  const float2 va = fma2(Ti, cpv, neg2(mul2(p.SK, ra)));
+  p.SK = fma2(vis, cpv, p.SK);
   p.T = Ti;
   const bool gm0 = c0 && !sk0, gm1 = c1 && !sk1;
   const bool gg0 = gm0 && og.x <= 0.999f, gg1 = gm1 && og.y <= 0.999f;
-  const float2 visg = make_float2(gm0 ? vis.x : 0.f, gm1 ? vis.y : 0.f);
+  // vis is zero where the pixel does not take the Gaussian; only the
+  // reference semantics drop contributors beyond that.
+  const float2 visg = REF ? make_float2(gm0 ? vis.x : 0.f, gm1 ? vis.y : 0.f) : vis;
   const float2 av = mul2(al, va);
   const float2 vs = make_float2(gg0 ? -av.x : 0.f, gg1 ? -av.y : 0.f);
-  const float2 vo = mul2(va, gs);
   const float2 vsdy = mul2(vs, dy);
   acc.m0 = add2(acc.m0, vs);
   acc.m1 = add2(acc.m1, vsdy);
   acc.m2 = fma2(vsdy, dy, acc.m2);
-  const float2 vxy0 = mul2(vs, fma2(f2(cb), dy, f2(adx)));
-  const float2 vxy1 = mul2(vs, fma2(f2(B.x), dy, f2(bdx)));
-  acc.ax += fabsf(vxy0.x) + fabsf(vxy0.y);
-  acc.ay += fabsf(vxy1.x) + fabsf(vxy1.y);
+  // |vs (a dx + b dy)| and |vs (b dx + c dy)| per pixel.
+  const float2 avs = make_float2(fabsf(vs.x), fabsf(vs.y));
+  const float2 g0 = fma2(f2(cb), dy, f2(adx)), g1 = fma2(f2(B.x), dy, f2(bdx));
+  acc.ax = fma2(avs, make_float2(fabsf(g0.x), fabsf(g0.y)), acc.ax);
+  acc.ay = fma2(avs, make_float2(fabsf(g1.x), fabsf(g1.y)), acc.ay);
   acc.cr = fma2(visg, p.vr, acc.cr);
   acc.cg = fma2(visg, p.vg, acc.cg);
   acc.cb = fma2(visg, p.vb, acc.cb);
-  acc.op = add2(acc.op, make_float2(gg0 ? vo.x : 0.f, gg1 ? vo.y : 0.f));
   acc.n += (gm0 ? 1u : 0u) + (gm1 ? 1u : 0u);
 }
 
@@ -802,11 +808,11 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           const float dx = esub(A.x, pcx);
           const float t1 = emul(emul(A.z, dx), dx);
           const float t2 = emul(A.w, dx);
-          const float cb = 0.5f * A.w;
+          const float cb = r0.w;  // the conic's b
           const float adx = A.z * dx, bdx = cb * dx;
           BwdAcc acc;
-          acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.op = f2(0.f);
-          acc.ax = acc.ay = 0.f;
+          acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = f2(0.f);
+          acc.ax = acc.ay = f2(0.f);
           acc.n = 0u;
           const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
           // The pairs of this warp whose 8x8 block had a pixel take the
@@ -841,21 +847,19 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           }
           const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
           float x[12];
-          x[0] = adx * M0 + cb * M1;
-          x[1] = bdx * M0 + B.x * M1;
-          x[2] = (0.5f * dx * dx) * M0;
+          x[0] = dx * M0;  // S1..S5 (the conic combination follows the CTA sum)
+          x[1] = M1;
+          x[2] = dx * x[0];
           x[3] = dx * M1;
-          x[4] = 0.5f * M2;
+          x[4] = M2;
           x[5] = acc.cr.x + acc.cr.y;
           x[6] = acc.cg.x + acc.cg.y;
           x[7] = acc.cb.x + acc.cb.y;
-          x[8] = acc.op.x + acc.op.y;
-          x[9] = acc.ax;
-          x[10] = acc.ay;
+          x[8] = M0;
+          x[9] = acc.ax.x + acc.ax.y;
+          x[10] = acc.ay.x + acc.ay.y;
           x[11] = (float)acc.n;
-          float r = warp_reduce_scatter12(x, lane);
-          // v_rgb is zero for a channel whose raw colour is negative.
-          if ((slot == 5 && Cc.x < 0.f) || (slot == 6 && Cc.y < 0.f) || (slot == 7 && Cc.z < 0.f)) r = 0.f;
+          const float r = warp_reduce_scatter12(x, lane);
           float* sp = reinterpret_cast<float*>(&s_part[warp][j][0]);
           if (writer) sp[slot] = r;
         }
@@ -878,6 +882,21 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
             f.y = f.y + g.y;
             f.z = f.z + g.z;
             f.w = f.w + g.w;
+          }
+        }
+        if (any) {
+          // The tile's S sums and sum vs into the screen-space gradients.
+          if (k == 0) {
+            const float4 r0 = s_rec[buf][j][0];
+            const float cc = s_rec[buf][j][1].x;
+            f = make_float4(r0.z * f.x + r0.w * f.y, r0.w * f.x + cc * f.y, 0.5f * f.z, f.w);
+          } else if (k == 1) {
+            // v_rgb is zero for a channel whose raw colour is negative.
+            const float4 r1 = s_rec[buf][j][1];
+            const float rb = s_rec[buf][j][2].x;
+            f = make_float4(0.5f * f.x, r1.z < 0.f ? 0.f : f.y, r1.w < 0.f ? 0.f : f.z, rb < 0.f ? 0.f : f.w);
+          } else {
+            f.x = f.x != 0.f ? -f.x / s_rec[buf][j][1].y : 0.f;
           }
         }
         if (a.det) {
