@@ -621,6 +621,7 @@ ORC_EXPORT void orc_sort_pairs_u32(const uint32_t* keys, const uint32_t* vals, u
   }
 }
 ORC_EXPORT float orc_expf(float x) { return portable_expf(x); }
+ORC_EXPORT float orc_blend_expf(float x) { return blend_expf(x); }
 ORC_EXPORT float orc_logf(float x) { return portable_logf(x); }
 
 // ---- forward ----

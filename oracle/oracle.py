@@ -40,6 +40,8 @@ def lib():
         L.orc_sort_pairs_u32.argtypes = [u32p, u32p, u32p, u32p, C.c_uint64]
         L.orc_expf.argtypes = [C.c_float]
         L.orc_expf.restype = C.c_float
+        L.orc_blend_expf.argtypes = [C.c_float]
+        L.orc_blend_expf.restype = C.c_float
         L.orc_logf.argtypes = [C.c_float]
         L.orc_logf.restype = C.c_float
         for suf, fp, ft in (("f32", f32p, C.c_float), ("f64", f64p, C.c_double)):
@@ -89,6 +91,10 @@ def expf(x):
 
 def logf(x):
     return lib().orc_logf(float(x))
+
+
+def blend_expf(x):
+    return lib().orc_blend_expf(float(x))
 
 
 class Forward:

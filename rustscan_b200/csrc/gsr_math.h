@@ -675,11 +675,17 @@ template <class F> GSR_HD V3<F> view_dir(const Cam<F>& cam, V3<F> mean) {
 // Per-pixel blend step (rasterize.wgsl:65-85).
 // ----------------------------------------------------------------------------
 // sigma = 0.5 * (a*dx*dx + 2*b*dx*dy + c*dy*dy) with d = mean - pixel centre,
-// each operation rounded on its own. blend_sigma_shared takes the two
-// per-column terms t1 = a*dx*dx and t2 = 2b*dx precomputed (kernels share
-// them between the pixels of a column).
+// evaluated left to right with the two multiply-adds contracted, as WGSL
+// lets an implementation do: t1 = (a*dx)*dx and t2 = (2b)*dx, then
+// 0.5 * fma((c*dy), dy, fma(t2, dy, t1)). Every other operation is rounded on
+// its own. The fused form is spelled out (fmaf on the host, the same fused
+// operation on the device), so host and device agree bit for bit whatever
+// the compiler contracts; it also lets the kernels run a pixel pair's sigma
+// as paired fused multiply-adds. blend_sigma_shared takes the per-column
+// terms t1 and t2 precomputed (kernels share them between the pixels of a
+// column).
 template <class F> GSR_HD F blend_sigma_shared(F t1, F t2, F dy, F cc) {
-  return emul(F(0.5), eadd(eadd(t1, emul(t2, dy)), emul(emul(cc, dy), dy)));
+  return emul(F(0.5), gfma(emul(cc, dy), dy, gfma(t2, dy, t1)));
 }
 template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
   return blend_sigma_shared(emul(emul(ca, dx), dx), emul(emul(F(2), cb), dx), dy, cc);
@@ -688,10 +694,11 @@ template <class F> GSR_HD F blend_sigma(F dx, F dy, F ca, F cb, F cc) {
 // exp(x) for the blend, where x = -sigma <= 0 matters (x > 0 only occurs
 // for sigma < 0, which the contribution test rejects whatever the value):
 // the reduction and polynomial of portable_expf, with n = round(x*log2(e))
-// taken by adding 1.5*2^23 (round-to-nearest-even, exact for |x*log2e| <
-// 2^22; its integer then sits in the low mantissa bits) and the scaling by
-// 2^n done by adding n to the exponent field, exact because the result stays
-// a normal number for x >= -87.33. Same IEEE operations on host and device.
+// taken by one fused multiply-add of 1.5*2^23 (round-to-nearest-even of the
+// exact product, for |x*log2e| < 2^22; its integer then sits in the low
+// mantissa bits) and the scaling by 2^n done by adding n to the exponent
+// field, exact because the result stays a normal number for x >= -87.33.
+// Same IEEE operations on host and device.
 // Constants of blend_expf (shared with the paired device version).
 namespace bexp {
 constexpr float kLog2e = 1.44269504088896341f;
@@ -710,7 +717,7 @@ constexpr float kLow = -87.3365f;                 // below: the result would not
 GSR_HD float blend_expf(float x) {
   x = fminf(x, 0.0f);
   if (!(x > bexp::kLow)) return (x != x) ? x : 0.0f;
-  const float t = eadd(emul(x, bexp::kLog2e), bexp::kMagic);
+  const float t = fmaf(x, bexp::kLog2e, bexp::kMagic);
   const float n = esub(t, bexp::kMagic);
   const int ni = (int)(float_to_bits(t) - bexp::kMagicBits);
   float r = fmaf(-n, bexp::kLn2Hi, x);

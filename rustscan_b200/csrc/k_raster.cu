@@ -217,14 +217,16 @@ __device__ __forceinline__ int build_list(const uint8_t* s_mask, uint32_t nb, ui
 // two-wide operations (fma2 is a fused multiply-add per half, add2 and mul2
 // round per half like the scalar operations).
 //
-// The compiler may contract a paired multiply feeding a paired add into one
-// fused multiply-add (even when written with explicit rounding), which would
-// change the blend decisions. So every multiply-then-add whose result decides
-// a contributor (sigma, and the range reduction of the exponential) runs as
-// individually rounded scalar operations, and the paired operations are used
-// only where contraction cannot occur (a product feeding a comparison, a
-// multiply-add that is fused by definition, a sum feeding a product) or in
-// gradient arithmetic, which has no bit-exactness requirement.
+// The compiler contracts a paired multiply feeding a paired add into one
+// fused multiply-add, even when written as PTX with .rn and with contraction
+// switched off (--fmad=false; measured: the paired and the fused results
+// agree bit for bit, the separately rounded scalar chain does not). The
+// decision arithmetic is therefore defined with its multiply-adds fused
+// (sigma and the range reduction of the exponential, gsr_math.h), and the
+// kernels spell those as fma2, which is then exact by construction; no
+// decision depends on a paired multiply feeding a paired add. The file is
+// built without contraction, like the CPU oracle, so that the remaining
+// scalar expressions keep their written rounding.
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -232,9 +234,9 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
 // blend_sigma_shared for the two pixels of a pair (same column: same t1,
-// t2), individually rounded scalar operations.
+// t2): the same operations in the same order, each half rounded on its own.
 __device__ __forceinline__ float2 sigma2(float t1, float t2, float2 dy, float cc) {
-  return make_float2(blend_sigma_shared(t1, t2, dy.x, cc), blend_sigma_shared(t1, t2, dy.y, cc));
+  return mul2(f2(0.5f), fma2(mul2(f2(cc), dy), dy, fma2(f2(t2), dy, f2(t1))));
 }
 
 // blend_expf(-sigma) for both pixels, without its range clamps: for every
@@ -244,9 +246,8 @@ __device__ __forceinline__ float2 sigma2(float t1, float t2, float2 dy, float cc
 // finite); every use of it is selected away by the pixel's contribution
 // flags, never multiplied in.
 __device__ __forceinline__ float2 blend_exp2(float2 sigma) {
-  const float xx = -sigma.x, xy = -sigma.y;
-  const float2 x = make_float2(xx, xy);
-  const float2 t = make_float2(eadd(emul(xx, bexp::kLog2e), bexp::kMagic), eadd(emul(xy, bexp::kLog2e), bexp::kMagic));
+  const float2 x = make_float2(-sigma.x, -sigma.y);
+  const float2 t = fma2(x, f2(bexp::kLog2e), f2(bexp::kMagic));
   const float2 n = add2(t, f2(-bexp::kMagic));
   const uint32_t ex = (__float_as_uint(t.x) - bexp::kMagicBits) << 23;
   const uint32_t ey = (__float_as_uint(t.y) - bexp::kMagicBits) << 23;
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_fwd_kernel(RasterArgs a) 
   #pragma unroll
             for (int k = 0; k < NP; ++k) {
               FwdPre& q = pre[u][k];
-              const float2 dy = make_float2(eadd(A.y, npcy[k].x), eadd(A.y, npcy[k].y));
+              const float2 dy = add2(f2(A.y), npcy[k]);
               q.sg = sigma2(t1, t2, dy, B.x);
               q.l0 = !(q.sg.x > B.y);
               q.l1 = !(q.sg.y > B.y);
@@ -590,7 +591,7 @@ __device__ __forceinline__ PairPre bwd_pair_pre(const BwdPair& p, float2 npcy, u
                                                 const float4& A, const float4& B) {
   PairPre q;
   const bool in0 = s < p.last0, in1 = s < p.last1;
-  q.dy = make_float2(eadd(A.y, npcy.x), eadd(A.y, npcy.y));
+  q.dy = add2(f2(A.y), npcy);
   q.sg = sigma2(t1, t2, q.dy, B.x);
   q.l0 = in0 && !(q.sg.x > B.y);
   q.l1 = in1 && !(q.sg.y > B.y);

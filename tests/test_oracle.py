@@ -56,6 +56,19 @@ def test_camera_projects_principal_point():
     np.testing.assert_allclose(fw.rec[0, :2], c["expected_pixel"], atol=c["tolerance"])
 
 
+def test_blend_exp_accuracy():
+    """The blend's exponential (fused range reduction, degree-7 polynomial)
+    over the range the contribution test can accept, sigma in [0, log(255) +
+    margin], and beyond it: within 2 ulp of exp."""
+    xs = np.concatenate([np.linspace(-8.0, 0.0, 40001), np.random.default_rng(1).uniform(-87.0, 0.0, 20000)])
+    worst = 0.0
+    for x in xs.astype(np.float32):
+        e = O.blend_expf(x)
+        ref = math.exp(float(x))
+        worst = max(worst, abs(e - ref) / float(np.spacing(np.float32(ref))))
+    assert worst <= 2.0, worst
+
+
 def test_portable_exp_log_accuracy():
     xs = np.concatenate([np.linspace(-87.3, 88.7, 20001), np.random.default_rng(0).uniform(-30, 5, 20000)])
     worst = 0.0
@@ -415,7 +428,8 @@ def _fma(a, b, c):
 
 def test_forward_blend_matches_independent_restatement():
     """The FP64 oracle's front-to-back blend against a restatement of
-    rasterize.wgsl:54-88 per pixel: sigma in the WGSL operation order,
+    rasterize.wgsl:54-88 per pixel: sigma in the WGSL operation order with
+    its two multiply-adds fused (as WGSL lets an implementation contract them),
     alpha = min(0.999, opacity * exp(-sigma)) taken when sigma >= 0 and
     alpha >= 1/255, colour += max(c, 0) * alpha * T as one fused multiply-add,
     T *= 1 - alpha, stop once T < 1e-4. Every output is compared bit for bit."""
@@ -440,7 +454,7 @@ def test_forward_blend_matches_independent_restatement():
                 mx, my, ca, cb, cc, op = (float(v) for v in f.rec[c, :6])
                 nv += 1
                 dx, dy = mx - pcx, my - pcy
-                sigma = 0.5 * ((ca * dx * dx + 2.0 * cb * dx * dy) + cc * dy * dy)
+                sigma = 0.5 * _fma(cc * dy, dy, _fma(2.0 * cb * dx, dy, ca * dx * dx))
                 alpha = min(0.999, op * math.exp(-sigma))
                 if not (sigma >= 0.0 and alpha >= 1.0 / 255.0):
                     continue
