@@ -42,6 +42,8 @@
 // Otherwise one CTA per item runs in item order.
 #include <algorithm>
 
+#include <type_traits>
+
 #include "gsr_kernels.h"
 
 namespace gsr {
@@ -249,8 +251,12 @@ __device__ __forceinline__ float2 blend_exp2(float2 sigma) {
   const float2 x = make_float2(-sigma.x, -sigma.y);
   const float2 t = fma2(x, f2(bexp::kLog2e), f2(bexp::kMagic));
   const float2 n = add2(t, f2(-bexp::kMagic));
-  const uint32_t ex = (__float_as_uint(t.x) - bexp::kMagicBits) << 23;
-  const uint32_t ey = (__float_as_uint(t.y) - bexp::kMagicBits) << 23;
+  // 2^n by exponent-field addition, as blend_expf: t's bits are those of
+  // 1.5 * 2^23 plus n, and a left shift by 23 drops the constant (its low 22
+  // bits are zero), leaving n << 23 modulo 2^32.
+  static_assert((bexp::kMagicBits << 23) == 0u, "the constant part shifts out");
+  const uint32_t ex = __float_as_uint(t.x) << 23;
+  const uint32_t ey = __float_as_uint(t.y) << 23;
   float2 r = fma2(neg2(n), f2(bexp::kLn2Hi), x);
   r = fma2(neg2(n), f2(bexp::kLn2Lo), r);
   float2 p = f2(bexp::kP7);
@@ -601,11 +607,12 @@ __device__ __forceinline__ PairPre bwd_pair_pre(const BwdPair& p, float2 npcy, u
 // The rest of the step: the contribution decisions repeat the forward's bit
 // for bit; the gradient follows blend_step_grad (rasterize_backwards, exact
 // adjoint), with the transmittance recovered with a Newton-refined hardware
-// reciprocal. Adds the pair's terms into acc. Straight-line code: a pixel
-// that does not take the Gaussian contributes zeros and keeps its state.
-// With REF (the reference semantics) a pixel whose transmittance fell to
-// 1e-4 no longer counts as a contributor and gets no gradient.
-template <bool REF>
+// reciprocal. Adds the pair's terms into acc (FIRST: sets acc to them).
+// Straight-line code: a pixel that does not take the Gaussian contributes
+// zeros and keeps its state. With REF (the reference semantics) a pixel
+// whose transmittance fell to 1e-4 no longer counts as a contributor and
+// gets no gradient.
+template <bool REF, bool FIRST>
 __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, float adx, float bdx, float cb,
                                               const float4& B, const float2 cpv, BwdAcc& acc) {
   const float2 dy = q.dy;
@@ -643,18 +650,32 @@ __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, floa
   const float2 av = mul2(al, va);
   const float2 vs = make_float2(gg0 ? -av.x : 0.f, gg1 ? -av.y : 0.f);
   const float2 vsdy = mul2(vs, dy);
-  acc.m0 = add2(acc.m0, vs);
-  acc.m1 = add2(acc.m1, vsdy);
-  acc.m2 = fma2(vsdy, dy, acc.m2);
   // |vs (a dx + b dy)| and |vs (b dx + c dy)| per pixel.
   const float2 avs = make_float2(fabsf(vs.x), fabsf(vs.y));
   const float2 g0 = fma2(f2(cb), dy, f2(adx)), g1 = fma2(f2(B.x), dy, f2(bdx));
-  acc.ax = fma2(avs, make_float2(fabsf(g0.x), fabsf(g0.y)), acc.ax);
-  acc.ay = fma2(avs, make_float2(fabsf(g1.x), fabsf(g1.y)), acc.ay);
-  acc.cr = fma2(visg, p.vr, acc.cr);
-  acc.cg = fma2(visg, p.vg, acc.cg);
-  acc.cb = fma2(visg, p.vb, acc.cb);
-  acc.n += (gm0 ? 1u : 0u) + (gm1 ? 1u : 0u);
+  const float2 ag0 = make_float2(fabsf(g0.x), fabsf(g0.y)), ag1 = make_float2(fabsf(g1.x), fabsf(g1.y));
+  const uint32_t nc = (gm0 ? 1u : 0u) + (gm1 ? 1u : 0u);
+  if constexpr (FIRST) {
+    acc.m0 = vs;
+    acc.m1 = vsdy;
+    acc.m2 = mul2(vsdy, dy);
+    acc.ax = mul2(avs, ag0);
+    acc.ay = mul2(avs, ag1);
+    acc.cr = mul2(visg, p.vr);
+    acc.cg = mul2(visg, p.vg);
+    acc.cb = mul2(visg, p.vb);
+    acc.n = nc;
+  } else {
+    acc.m0 = add2(acc.m0, vs);
+    acc.m1 = add2(acc.m1, vsdy);
+    acc.m2 = fma2(vsdy, dy, acc.m2);
+    acc.ax = fma2(avs, ag0, acc.ax);
+    acc.ay = fma2(avs, ag1, acc.ay);
+    acc.cr = fma2(visg, p.vr, acc.cr);
+    acc.cg = fma2(visg, p.vg, acc.cg);
+    acc.cb = fma2(visg, p.vb, acc.cb);
+    acc.n += nc;
+  }
 }
 
 // Maps the forward's per-entry warp-block bits (blocks of kFwdPPL pixels
@@ -748,6 +769,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     uint32_t wsel = 0;  // the forward blocks inside this warp's block
   #pragma unroll
     for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
+    const uint32_t b0 = fwd_block_of<TW, PPL>(warp, 0);
     auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
     // List entries [lo, hi) of a batch into registers.
     uint32_t pc[kSI], ph[kSI];
@@ -811,40 +833,41 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           const float t2 = emul(A.w, dx);
           const float cb = r0.w;  // the conic's b
           const float adx = A.z * dx, bdx = cb * dx;
-          BwdAcc acc;
-          acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = f2(0.f);
-          acc.ax = acc.ay = f2(0.f);
-          acc.n = 0u;
+          BwdAcc acc;  // set by the first pair evaluated
           const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
           // The pairs of this warp whose 8x8 block had a pixel take the
           // Gaussian in the forward (the others contribute nothing here).
           const uint32_t mraw = s_mask[buf][j];
-          uint32_t need = 0;
-  #pragma unroll
-          for (int k = 0; k < NP; ++k)
-            if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) need |= 1u << k;
-          // The needed pairs run as one straight-line block (need is
-          // warp-uniform), so that their independent chains interleave.
-          auto rest = [&](int k) {
+          // The needed pairs run as one straight-line block (warp-uniform),
+          // so that their independent chains interleave; the first one
+          // evaluated initialises the sums.
+          auto rest = [&](int k, auto first) {
             const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
             const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
             const float2 cpv =
                 fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
-            bwd_pair_rest<REF>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
+            bwd_pair_rest<REF, decltype(first)::value>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
           };
+          constexpr std::integral_constant<bool, true> kFirst{};
+          constexpr std::integral_constant<bool, false> kNext{};
           if constexpr (NP == 2) {
-            if (need == 3u) {
-              rest(0);
-              rest(1);
+            // Pair k of this warp lies in forward block b0 + k * KX.
+            constexpr uint32_t KX = TW / 8, both = 1u | (1u << KX);
+            const uint32_t need = (mraw >> b0) & both;  // listed entries have at least one
+            if (need == both) {
+              rest(0, kFirst);
+              rest(1, kNext);
             } else if (need == 1u) {
-              rest(0);
-            } else if (need == 2u) {
-              rest(1);
+              rest(0, kFirst);
+            } else {
+              rest(1, kFirst);
             }
           } else {
+            acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.ax = acc.ay = f2(0.f);
+            acc.n = 0u;
   #pragma unroll
             for (int k = 0; k < NP; ++k)
-              if (need & (1u << k)) rest(k);
+              if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) rest(k, kNext);
           }
           const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
           float x[12];
