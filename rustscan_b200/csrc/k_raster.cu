@@ -259,12 +259,11 @@ __device__ __forceinline__ float2 blend_exp2(float2 sigma) {
   const uint32_t ey = __float_as_uint(t.y) << 23;
   float2 r = fma2(neg2(n), f2(bexp::kLn2Hi), x);
   r = fma2(neg2(n), f2(bexp::kLn2Lo), r);
-  float2 p = f2(bexp::kP7);
-  p = fma2(p, r, f2(bexp::kP6));
-  p = fma2(p, r, f2(bexp::kP5));
-  p = fma2(p, r, f2(bexp::kP4));
-  p = fma2(p, r, f2(bexp::kP3));
-  p = fma2(p, r, f2(0.5f));
+  float2 p = f2(bexp::kC6);
+  p = fma2(p, r, f2(bexp::kC5));
+  p = fma2(p, r, f2(bexp::kC4));
+  p = fma2(p, r, f2(bexp::kC3));
+  p = fma2(p, r, f2(bexp::kC2));
   p = fma2(p, r, f2(1.0f));
   p = fma2(p, r, f2(1.0f));
   return make_float2(__uint_as_float(__float_as_uint(p.x) + ex), __uint_as_float(__float_as_uint(p.y) + ey));
