@@ -30,7 +30,7 @@ WORKLOAD = "batched training step: 1,000,000 Gaussians, SH degree 3, 8 views of 
 # ncu smsp__inst_executed.sum of the raster kernels on one 1280x720 view of
 # this workload (6,273,269 intersections), per intersection
 # (profiles/raster_c3_1view_issue.md).
-WARP_INST_PER_ISECT = {"raster_bwd": 176.72e6 / 6273269, "raster_fwd": 136.09e6 / 6273269}
+WARP_INST_PER_ISECT = {"raster_bwd": 153.95e6 / 6273269, "raster_fwd": 134.88e6 / 6273269}
 
 
 def parse():

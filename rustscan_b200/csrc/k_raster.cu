@@ -50,12 +50,13 @@ namespace gsr {
 
 namespace {
 
-// Pixels per lane. The forward gains nothing from more than 2; the
-// backward amortises its per-Gaussian warp reduction over twice the pixels
-// with 4 where the tile is tall enough for an 8 x 16 warp block (16x16).
+// Pixels per lane. The forward gains nothing from more than 2. The
+// backward of 16x16 tiles runs one warp per tile with 8 pixels per lane
+// (raster_bwd_tile_kernel), so that each Gaussian's warp reduction serves
+// the whole tile; the other tile shapes run raster_bwd_kernel with 2.
 constexpr int kFwdPPL = 2;
 static_assert(4 * kFwdPPL == 8, "forward warp blocks, and so the exported hit bits, are 8x8 pixels");
-constexpr int kBwdPPL16 = 4;
+constexpr int kBwdPPL = 2;
 
 struct RasterArgs {
   ViewSet vs;
@@ -578,8 +579,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // opacity * G, so the opacity-path gradient sum va * G over those pixels is
 // -(sum vs) / opacity: M0 serves for both. The absolute mean-gradient sums
 // (densification statistics) stay per pixel.
-struct BwdAcc {
+struct BwdMom {
   float2 m0, m1, m2;
+};
+struct BwdAcc {
   float2 cr, cg, cb;  // colour gradients
   float2 ax, ay;      // sums of |d/dx| and |d/dy| of the per-pixel mean gradients
   uint32_t n;         // contributing pixels
@@ -606,14 +609,15 @@ __device__ __forceinline__ PairPre bwd_pair_pre(const BwdPair& p, float2 npcy, u
 // The rest of the step: the contribution decisions repeat the forward's bit
 // for bit; the gradient follows blend_step_grad (rasterize_backwards, exact
 // adjoint), with the transmittance recovered with a Newton-refined hardware
-// reciprocal. Adds the pair's terms into acc (FIRST: sets acc to them).
-// Straight-line code: a pixel that does not take the Gaussian contributes
-// zeros and keeps its state. With REF (the reference semantics) a pixel
-// whose transmittance fell to 1e-4 no longer counts as a contributor and
-// gets no gradient.
-template <bool REF, bool FIRST>
+// reciprocal. Adds the pair's terms into mom and acc (FIRST_MOM, FIRST_ACC:
+// sets them to the terms). Straight-line code: a pixel that does not take
+// the Gaussian contributes zeros and keeps its state. With REF (the
+// reference semantics) a pixel whose transmittance fell to 1e-4 no longer
+// counts as a contributor and gets no gradient.
+template <bool REF, bool FIRST_MOM, bool FIRST_ACC>
 __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, float adx, float bdx, float cb,
-                                              const float4& B, const float2 cpv, BwdAcc& acc) {
+                                              const float4& B, const float2 cpv, const float2 vr, const float2 vg,
+                                              const float2 vb, BwdMom& mom, BwdAcc& acc) {
   const float2 dy = q.dy;
   const float2 gs = blend_exp2(q.sg);
   const float2 og = mul2(f2(B.z), gs);
@@ -654,25 +658,28 @@ __device__ __forceinline__ void bwd_pair_rest(BwdPair& p, const PairPre& q, floa
   const float2 g0 = fma2(f2(cb), dy, f2(adx)), g1 = fma2(f2(B.x), dy, f2(bdx));
   const float2 ag0 = make_float2(fabsf(g0.x), fabsf(g0.y)), ag1 = make_float2(fabsf(g1.x), fabsf(g1.y));
   const uint32_t nc = (gm0 ? 1u : 0u) + (gm1 ? 1u : 0u);
-  if constexpr (FIRST) {
-    acc.m0 = vs;
-    acc.m1 = vsdy;
-    acc.m2 = mul2(vsdy, dy);
+  if constexpr (FIRST_MOM) {
+    mom.m0 = vs;
+    mom.m1 = vsdy;
+    mom.m2 = mul2(vsdy, dy);
+  } else {
+    mom.m0 = add2(mom.m0, vs);
+    mom.m1 = add2(mom.m1, vsdy);
+    mom.m2 = fma2(vsdy, dy, mom.m2);
+  }
+  if constexpr (FIRST_ACC) {
     acc.ax = mul2(avs, ag0);
     acc.ay = mul2(avs, ag1);
-    acc.cr = mul2(visg, p.vr);
-    acc.cg = mul2(visg, p.vg);
-    acc.cb = mul2(visg, p.vb);
+    acc.cr = mul2(visg, vr);
+    acc.cg = mul2(visg, vg);
+    acc.cb = mul2(visg, vb);
     acc.n = nc;
   } else {
-    acc.m0 = add2(acc.m0, vs);
-    acc.m1 = add2(acc.m1, vsdy);
-    acc.m2 = fma2(vsdy, dy, acc.m2);
     acc.ax = fma2(avs, ag0, acc.ax);
     acc.ay = fma2(avs, ag1, acc.ay);
-    acc.cr = fma2(visg, p.vr, acc.cr);
-    acc.cg = fma2(visg, p.vg, acc.cg);
-    acc.cb = fma2(visg, p.vb, acc.cb);
+    acc.cr = fma2(visg, vr, acc.cr);
+    acc.cg = fma2(visg, vg, acc.cg);
+    acc.cb = fma2(visg, vb, acc.cb);
     acc.n += nc;
   }
 }
@@ -768,7 +775,6 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     uint32_t wsel = 0;  // the forward blocks inside this warp's block
   #pragma unroll
     for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
-    const uint32_t b0 = fwd_block_of<TW, PPL>(warp, 0);
     auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
     // List entries [lo, hi) of a batch into registers.
     uint32_t pc[kSI], ph[kSI];
@@ -832,43 +838,35 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           const float t2 = emul(A.w, dx);
           const float cb = r0.w;  // the conic's b
           const float adx = A.z * dx, bdx = cb * dx;
-          BwdAcc acc;  // set by the first pair evaluated
+          BwdMom mom;  // set by the first pair evaluated
+          BwdAcc acc;
           const float cp0 = fmaxf(Cc.x, 0.f), cp1 = fmaxf(Cc.y, 0.f), cp2 = fmaxf(Cc.z, 0.f);
           // The pairs of this warp whose 8x8 block had a pixel take the
           // Gaussian in the forward (the others contribute nothing here).
           const uint32_t mraw = s_mask[buf][j];
-          // The needed pairs run as one straight-line block (warp-uniform),
-          // so that their independent chains interleave; the first one
-          // evaluated initialises the sums.
+          // Pair k takes part when its forward block took the Gaussian (a
+          // warp-uniform test); with one pair per lane the first pair sets
+          // the sums.
           auto rest = [&](int k, auto first) {
             const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
             const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
             const float2 cpv =
                 fma2(f2(cp2), pp[k].vb, fma2(f2(cp1), pp[k].vg, mul2(f2(cp0), pp[k].vr)));
-            bwd_pair_rest<REF, decltype(first)::value>(pp[k], pre, adx, bdx, cb, B, cpv, acc);
+            constexpr bool kF = decltype(first)::value;
+            bwd_pair_rest<REF, kF, kF>(pp[k], pre, adx, bdx, cb, B, cpv, pp[k].vr, pp[k].vg, pp[k].vb, mom, acc);
           };
           constexpr std::integral_constant<bool, true> kFirst{};
           constexpr std::integral_constant<bool, false> kNext{};
-          if constexpr (NP == 2) {
-            // Pair k of this warp lies in forward block b0 + k * KX.
-            constexpr uint32_t KX = TW / 8, both = 1u | (1u << KX);
-            const uint32_t need = (mraw >> b0) & both;  // listed entries have at least one
-            if (need == both) {
-              rest(0, kFirst);
-              rest(1, kNext);
-            } else if (need == 1u) {
-              rest(0, kFirst);
-            } else {
-              rest(1, kFirst);
-            }
+          if constexpr (NP == 1) {
+            rest(0, kFirst);  // listed entries take part in the warp's one pair
           } else {
-            acc.m0 = acc.m1 = acc.m2 = acc.cr = acc.cg = acc.cb = acc.ax = acc.ay = f2(0.f);
+            mom.m0 = mom.m1 = mom.m2 = acc.cr = acc.cg = acc.cb = acc.ax = acc.ay = f2(0.f);
             acc.n = 0u;
   #pragma unroll
             for (int k = 0; k < NP; ++k)
               if ((mraw >> fwd_block_of<TW, PPL>(warp, k)) & 1u) rest(k, kNext);
           }
-          const float M0 = acc.m0.x + acc.m0.y, M1 = acc.m1.x + acc.m1.y, M2 = acc.m2.x + acc.m2.y;
+          const float M0 = mom.m0.x + mom.m0.y, M1 = mom.m1.x + mom.m1.y, M2 = mom.m2.x + mom.m2.y;
           float x[12];
           x[0] = dx * M0;  // S1..S5 (the conic combination follows the CTA sum)
           x[1] = M1;
@@ -948,6 +946,226 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
   }
 }
 
+// The backward of 16x16 tiles with one warp per tile. Lane l owns, in each
+// of the tile's four 8x8 blocks q (block column q & 1, block row q >> 1), the
+// pixel pair (8 (q & 1) + (l & 7), 8 (q >> 1) + (l >> 3) + {0, 4}), so that
+// pair q lies in the forward's warp block q and an entry's block bits say
+// which pairs need it. Against two warps per tile, each list entry is staged,
+// set up and reduced once per tile rather than once per warp whose block it
+// reaches, and the tile's sum needs no second warp. The pairs of a block
+// column share dx and the terms that depend on it; the sigma-gradient
+// moments are kept per column (S1 = dx0 M0_0 + dx1 M0_1 and so on).
+template <int BATCH, bool REF>
+__global__ void __launch_bounds__(32, 16) raster_bwd_tile_kernel(RasterArgs a) {
+  constexpr int NT = 32;
+  constexpr int kSI = BATCH / NT;  // entries a lane stages per batch
+  static_assert(BATCH % NT == 0, "whole batches per lane");
+  __shared__ float4 s_rec[2][BATCH][3];  // raw records
+  __shared__ uint32_t s_cidx[2][BATCH];
+  __shared__ uint8_t s_mask[2][BATCH];  // forward blocks that take the entry
+  __shared__ uint16_t s_list[BATCH];
+  __shared__ float4 s_part[BATCH][3];   // the tile's reduced sums of listed entries
+  __shared__ float2 s_v[4][3][32];      // upstream colour gradient of each lane's pairs (read only)
+  __shared__ uint32_t s_item;
+  __shared__ CostListView s_lists;
+  load_cost_lists(a, &s_lists);
+  const int lane = threadIdx.x;
+  const int slot = reduce12_slot(lane);                          // the gradient value this lane ends with
+  const bool writer = (lane & 1) == 0 && !((lane & 2) && (lane & 4));  // one lane per value
+  for (uint32_t round = 0;; ++round) {
+    const uint32_t item = next_item(a, round, &s_item, &s_lists);
+    if (item == kNoItem) break;
+    const uint32_t v = find_view(a.vs, item);
+    const ViewDesc& vd = a.vs.views[v];
+    const uint32_t t = item - vd.tile_base;
+    const uint32_t tx = t % vd.tiles_x, ty = t / vd.tiles_x;
+    const uint32_t px0 = tx * 16 + (lane & 7), py0 = ty * 16 + (lane >> 3);
+    const float pcx0 = (float)px0 + 0.5f, pcx1 = (float)(px0 + 8) + 0.5f;
+    // Negated pixel-centre rows of the lane's pairs: block row h, half u at
+    // row py0 + 8 h + 4 u (small integers plus 0.5: exact).
+    const float npy[4] = {-((float)py0 + 0.5f), -((float)(py0 + 4) + 0.5f), -((float)(py0 + 8) + 0.5f),
+                          -((float)(py0 + 12) + 0.5f)};
+    const uint32_t* ranges = slice(a.b.ranges, 2 * a.b.Tcap, v);
+    const uint32_t s0 = ranges[2 * t];
+    const uint32_t* vals = isect_index_src(a.b, v);
+    const uint32_t vmask = isect_index_mask(a.b);
+    const float4* rec = slice(a.b.rec, a.b.Vcap * 3, v);
+    const uint8_t* hitw = slice(a.b.hitw, a.b.Icap, v);
+    float4* sgrad = slice(a.b.sgrad, a.b.Vcap * 3, v);
+    float* part = a.b.sgrad_part + (size_t)a.b.Icap * 12 * v;
+    BwdPair pp[4];
+    uint32_t mylast = 0;
+  #pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      load_bwd_pair(a, vd, v, px0 + 8 * (q & 1), py0 + 8 * (q >> 1), pp[q]);
+      mylast = max(mylast, max(pp[q].last0, pp[q].last1));
+      s_v[q][0][lane] = pp[q].vr;  // kept in shared memory, not registers
+      s_v[q][1][lane] = pp[q].vg;
+      s_v[q][2][lane] = pp[q].vb;
+    }
+    const uint32_t smax = __reduce_max_sync(0xffffffffu, mylast);
+    auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
+    uint32_t pc[kSI], ph[kSI];
+    auto fetch = [&](uint32_t lo, uint32_t hi) {
+  #pragma unroll
+      for (int it = 0; it < kSI; ++it) {
+        const uint32_t s = lo + lane + it * NT;
+        const bool ok = s < hi;
+        ph[it] = ok ? hitw[s] : 0u;
+        pc[it] = ok ? (vals[s] & vmask) : 0u;
+      }
+    };
+    auto issue = [&](uint32_t lo, uint32_t hi, int buf) {
+  #pragma unroll
+      for (int it = 0; it < kSI; ++it) {
+        const uint32_t j = lane + it * NT;
+        if (lo + j < hi) {
+          s_mask[buf][j] = (uint8_t)ph[it];
+          if (ph[it]) {
+            s_cidx[buf][j] = pc[it];
+            const float4* r = rec + (size_t)pc[it] * 3;
+            cp_async16(&s_rec[buf][j][0], r);
+            cp_async16(&s_rec[buf][j][1], r + 1);
+            cp_async16(&s_rec[buf][j][2], r + 2);
+          }
+        }
+      }
+      cp_async_commit();
+    };
+    uint32_t be = smax, bs = be > s0 ? batch_lo(be) : s0;
+    if (be > s0) {
+      fetch(bs, be);
+      issue(bs, be, 0);
+    }
+    uint32_t nbe = bs, nbs = nbe > s0 ? batch_lo(nbe) : s0;
+    if (nbe > s0) fetch(nbs, nbe);
+    int buf = 0;
+    while (be > s0) {
+      const uint32_t nb = be - bs;
+      if (nbe > s0)
+        issue(nbs, nbe, buf ^ 1);
+      else
+        cp_async_commit();
+      const uint32_t n2e = nbs, n2s = n2e > s0 ? batch_lo(n2e) : s0;
+      if (n2e > s0) fetch(n2s, n2e);
+      cp_async_wait1();  // this lane's copies of the current batch have landed
+      __syncthreads();   // and every lane's
+      const int cnt = build_list(s_mask[buf], nb, 0xfu, lane, s_list);
+      for (int e = cnt - 1; e >= 0; --e) {
+        const uint32_t j = s_list[e];
+        const uint32_t s = bs + j;
+        const float4 r0 = s_rec[buf][j][0], r1 = s_rec[buf][j][1], r2 = s_rec[buf][j][2];
+        const float4 A = make_float4(r0.x, r0.y, r0.z, 2.f * r0.w);  // 2b is exact
+        const float4 B = make_float4(r1.x, r2.y + kRejectMargin, r1.y, 0.f);
+        const float cb = r0.w;  // the conic's b
+        const float cp0 = fmaxf(r1.z, 0.f), cp1 = fmaxf(r1.w, 0.f), cp2 = fmaxf(r2.x, 0.f);
+        const uint32_t need = s_mask[buf][j];  // bit q: pair q takes part
+        const float dx0 = esub(A.x, pcx0), dx1 = esub(A.x, pcx1);
+        BwdMom mom0, mom1;
+        BwdAcc acc;
+        constexpr std::integral_constant<bool, true> kT{};
+        constexpr std::integral_constant<bool, false> kF{};
+        // The pairs of block column c (q = c upper, q = c + 2 lower) as one
+        // straight-line block; FM: the column's first pair sets its moments,
+        // FA: the entry's first pair sets the shared sums.
+        auto column = [&](auto cc, auto fa, BwdMom& mom) {
+          constexpr int c = decltype(cc)::value;
+          constexpr bool FA = decltype(fa)::value;
+          const float dx = c ? dx1 : dx0;
+          const float t1 = emul(emul(A.z, dx), dx);
+          const float t2 = emul(A.w, dx);
+          const float adx = A.z * dx, bdx = cb * dx;
+          auto rest = [&](auto qq, auto fm, auto fa2) {
+            constexpr int q = decltype(qq)::value;
+            const float2 npcy = make_float2(npy[2 * (q >> 1)], npy[2 * (q >> 1) + 1]);
+            const PairPre pre = bwd_pair_pre(pp[q], npcy, s, t1, t2, A, B);
+            const float2 vr = s_v[q][0][lane], vg = s_v[q][1][lane], vb = s_v[q][2][lane];
+            const float2 cpv = fma2(f2(cp2), vb, fma2(f2(cp1), vg, mul2(f2(cp0), vr)));
+            bwd_pair_rest<REF, decltype(fm)::value, decltype(fa2)::value>(pp[q], pre, adx, bdx, cb, B, cpv, vr, vg,
+                                                                          vb, mom, acc);
+          };
+          const uint32_t nc = (need >> c) & 5u;  // bit 0: upper pair, bit 2: lower pair
+          if (nc == 5u) {
+            rest(std::integral_constant<int, c>{}, kT, std::integral_constant<bool, FA>{});
+            rest(std::integral_constant<int, c + 2>{}, kF, kF);
+          } else if (nc == 1u) {
+            rest(std::integral_constant<int, c>{}, kT, std::integral_constant<bool, FA>{});
+          } else {
+            rest(std::integral_constant<int, c + 2>{}, kT, std::integral_constant<bool, FA>{});
+          }
+        };
+        if (need & 5u) {
+          column(std::integral_constant<int, 0>{}, kT, mom0);
+        } else {
+          mom0.m0 = mom0.m1 = mom0.m2 = acc.cr = acc.cg = acc.cb = acc.ax = acc.ay = f2(0.f);
+          acc.n = 0u;
+        }
+        if (need & 10u)
+          column(std::integral_constant<int, 1>{}, kF, mom1);
+        else
+          mom1.m0 = mom1.m1 = mom1.m2 = f2(0.f);
+        const float M00 = mom0.m0.x + mom0.m0.y, M01 = mom1.m0.x + mom1.m0.y;
+        const float M10 = mom0.m1.x + mom0.m1.y, M11 = mom1.m1.x + mom1.m1.y;
+        const float e0 = dx0 * M00, e1 = dx1 * M01;
+        float x[12];
+        x[0] = e0 + e1;  // S1..S5 (the conic combination follows the reduction)
+        x[1] = M10 + M11;
+        x[2] = dx0 * e0 + dx1 * e1;
+        x[3] = dx0 * M10 + dx1 * M11;
+        x[4] = (mom0.m2.x + mom0.m2.y) + (mom1.m2.x + mom1.m2.y);
+        x[5] = acc.cr.x + acc.cr.y;
+        x[6] = acc.cg.x + acc.cg.y;
+        x[7] = acc.cb.x + acc.cb.y;
+        x[8] = M00 + M01;
+        x[9] = acc.ax.x + acc.ax.y;
+        x[10] = acc.ay.x + acc.ay.y;
+        x[11] = (float)acc.n;
+        const float r = warp_reduce_scatter12(x, lane);
+        if (writer) reinterpret_cast<float*>(&s_part[j][0])[slot] = r;
+      }
+      __syncwarp();
+      for (uint32_t qi = lane; qi < nb * 3; qi += NT) {
+        const uint32_t j = qi / 3, k = qi % 3;
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (s_mask[buf][j]) {
+          f = s_part[j][k];
+          if (k == 0) {
+            const float4 r0 = s_rec[buf][j][0];
+            const float cc = s_rec[buf][j][1].x;
+            f = make_float4(r0.z * f.x + r0.w * f.y, r0.w * f.x + cc * f.y, 0.5f * f.z, f.w);
+          } else if (k == 1) {
+            // v_rgb is zero for a channel whose raw colour is negative.
+            const float4 r1 = s_rec[buf][j][1];
+            const float rb = s_rec[buf][j][2].x;
+            f = make_float4(0.5f * f.x, r1.z < 0.f ? 0.f : f.y, r1.w < 0.f ? 0.f : f.z, rb < 0.f ? 0.f : f.w);
+          } else {
+            f.x = f.x != 0.f ? -f.x / s_rec[buf][j][1].y : 0.f;
+          }
+        }
+        if (a.det) {
+          reinterpret_cast<float4*>(part + (size_t)(bs + j) * 12)[k] = f;
+        } else if (f.x != 0.f || f.y != 0.f || f.z != 0.f || f.w != 0.f) {
+          atomicAdd(sgrad + (size_t)s_cidx[buf][j] * 3 + k, f);
+        }
+      }
+      __syncthreads();  // the next batch's copies reuse this buffer
+      be = bs;
+      bs = nbs;
+      nbe = n2e;
+      nbs = n2s;
+      buf ^= 1;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may outlive the block
+    if (a.det) {
+      const uint32_t s1 = ranges[2 * t + 1];
+      for (uint32_t s = smax > s0 ? smax : s0; s + lane < s1; s += NT) {
+        float4* p4 = reinterpret_cast<float4*>(part + (size_t)(s + lane) * 12);
+        p4[0] = p4[1] = p4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
+}
+
 // Gaussians per shared-memory batch: 0 selects the tuned defaults (128 in
 // the forward, 64 in the backward); other values round up to 64, 128 or 256.
 // The backward of shapes with two or more warps per tile caps at 128 (its
@@ -1009,10 +1227,22 @@ cudaError_t launch_bwd_mode(const RasterArgs& a, uint32_t batch, int num_sms, cu
       return launch_items<raster_bwd_kernel<TW, TH, PPL, (kMaxBatch > 128 ? 256 : 128), REF>>(NT, a, num_sms, st);
   }
 }
+// The 16x16 backward stages 64 entries per batch whatever the forward's
+// batch: 13 KB of shared memory and at most 128 registers per one-warp CTA
+// let 16 CTAs share an SM (a 128-entry batch would fit 9).
+template <bool REF>
+cudaError_t launch_bwd_tile16(const RasterArgs& a, int num_sms, cudaStream_t st) {
+  return launch_items<raster_bwd_tile_kernel<64, REF>>(32, a, num_sms, st);
+}
 template <int TW, int TH, int PPL>
 cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
-  return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, batch, num_sms, st)
-                    : launch_bwd_mode<TW, TH, PPL, false>(a, batch, num_sms, st);
+  if constexpr (TW == 16 && TH == 16) {
+    (void)batch;
+    return a.ref_mode ? launch_bwd_tile16<true>(a, num_sms, st) : launch_bwd_tile16<false>(a, num_sms, st);
+  } else {
+    return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, batch, num_sms, st)
+                      : launch_bwd_mode<TW, TH, PPL, false>(a, batch, num_sms, st);
+  }
 }
 
 }  // namespace
@@ -1025,13 +1255,13 @@ void raster_warm_up(uint32_t tile_w, uint32_t tile_h, uint32_t batch, int num_sm
     a.ref_mode = ref;
     if (tile_w == 16 && tile_h == 16) {
       (void)launch_fwd_shape<16, 16, kFwdPPL>(a, batch, num_sms, nullptr);
-      (void)launch_bwd_shape<16, 16, kBwdPPL16>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<16, 16, kBwdPPL>(a, batch, num_sms, nullptr);
     } else if (tile_w == 8 && tile_h == 8) {
       (void)launch_fwd_shape<8, 8, kFwdPPL>(a, batch, num_sms, nullptr);
-      (void)launch_bwd_shape<8, 8, 2>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<8, 8, kBwdPPL>(a, batch, num_sms, nullptr);
     } else if (tile_w == 32 && tile_h == 8) {
       (void)launch_fwd_shape<32, 8, kFwdPPL>(a, batch, num_sms, nullptr);
-      (void)launch_bwd_shape<32, 8, 2>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<32, 8, kBwdPPL>(a, batch, num_sms, nullptr);
     }
   }
 }
@@ -1084,9 +1314,9 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     cudaError_t e = cudaMemsetAsync(b.sched_ticket, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
   }
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL16>(a, vs.batch, s.num_sms, st);
-  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, 2>(a, vs.batch, s.num_sms, st);
-  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, 2>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, kBwdPPL>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, kBwdPPL>(a, vs.batch, s.num_sms, st);
   return cudaErrorInvalidValue;
 }
 
