@@ -72,7 +72,8 @@ typedef struct gsr_config {
   float background[3];     /* background colour (0,0,0) */
   uint32_t tile_w, tile_h; /* tile shape: 16x16 (default), 8x8 or 32x8 */
   uint32_t batch;          /* Gaussians staged in shared memory per raster batch: 64, 128 or 256
-                              (rounded up; 0: tuned defaults, 128 forward / 64 backward) */
+                              (rounded up; 0: tuned defaults, 128 forward / 64 backward; the
+                              16x16 backward always stages 64) */
   int32_t sh_dtype;        /* GSR_SH_F32 or GSR_SH_BF16 storage of SH coefficients */
   int32_t adjoint;         /* GSR_ADJOINT_EXACT (default) or GSR_ADJOINT_REFERENCE */
   int32_t deterministic;   /* 1: fixed-order gradient reduction, bitwise reruns */
