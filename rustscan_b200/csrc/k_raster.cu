@@ -52,11 +52,18 @@ namespace {
 
 // Pixels per lane. The forward gains nothing from more than 2. The
 // backward of 16x16 tiles runs one warp per tile with 8 pixels per lane
-// (raster_bwd_tile_kernel), so that each Gaussian's warp reduction serves
-// the whole tile; the other tile shapes run raster_bwd_kernel with 2.
+// (raster_bwd_tile_kernel) when the launch has tiles enough to fill the
+// GPU several times over with one-warp CTAs, so that each Gaussian's warp
+// reduction serves the whole tile; otherwise two warps per tile with 4
+// pixels per lane (raster_bwd_kernel), which keeps twice the warps busy on a
+// small view. The other tile shapes run raster_bwd_kernel with 2.
 constexpr int kFwdPPL = 2;
 static_assert(4 * kFwdPPL == 8, "forward warp blocks, and so the exported hit bits, are 8x8 pixels");
 constexpr int kBwdPPL = 2;
+constexpr int kBwdPPL16 = 4;
+// One-warp CTA waves (the tile kernel's residency times the SMs) a launch
+// must fill before the 16x16 backward runs one warp per tile.
+constexpr uint32_t kTileKernelWaves = 4;
 
 struct RasterArgs {
   ViewSet vs;
@@ -775,6 +782,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
     uint32_t wsel = 0;  // the forward blocks inside this warp's block
   #pragma unroll
     for (int k = 0; k < NP; ++k) wsel |= 1u << fwd_block_of<TW, PPL>(warp, k);
+    const uint32_t b0 = fwd_block_of<TW, PPL>(warp, 0);
     auto batch_lo = [&](uint32_t e) { return (e - s0 > (uint32_t)BATCH) ? e - BATCH : s0; };
     // List entries [lo, hi) of a batch into registers.
     uint32_t pc[kSI], ph[kSI];
@@ -845,8 +853,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           // Gaussian in the forward (the others contribute nothing here).
           const uint32_t mraw = s_mask[buf][j];
           // Pair k takes part when its forward block took the Gaussian (a
-          // warp-uniform test); with one pair per lane the first pair sets
-          // the sums.
+          // warp-uniform test); the first pair evaluated sets the sums.
           auto rest = [&](int k, auto first) {
             const float2 npcy = make_float2(-((float)(pyb + 8 * k) + 0.5f), -((float)(pyb + 8 * k + 4) + 0.5f));
             const PairPre pre = bwd_pair_pre(pp[k], npcy, s, t1, t2, A, B);
@@ -859,6 +866,20 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
           constexpr std::integral_constant<bool, false> kNext{};
           if constexpr (NP == 1) {
             rest(0, kFirst);  // listed entries take part in the warp's one pair
+          } else if constexpr (NP == 2) {
+            // Pair k of this warp lies in forward block b0 + k * KX; the
+            // needed pairs run as one straight-line block, so that their
+            // independent chains interleave.
+            constexpr uint32_t KX = TW / 8, both = 1u | (1u << KX);
+            const uint32_t need = (mraw >> b0) & both;  // listed entries have at least one
+            if (need == both) {
+              rest(0, kFirst);
+              rest(1, kNext);
+            } else if (need == 1u) {
+              rest(0, kFirst);
+            } else {
+              rest(1, kFirst);
+            }
           } else {
             mom.m0 = mom.m1 = mom.m2 = acc.cr = acc.cg = acc.cb = acc.ax = acc.ay = f2(0.f);
             acc.n = 0u;
@@ -1236,13 +1257,15 @@ cudaError_t launch_bwd_tile16(const RasterArgs& a, int num_sms, cudaStream_t st)
 }
 template <int TW, int TH, int PPL>
 cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
-  if constexpr (TW == 16 && TH == 16) {
-    (void)batch;
+  return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, batch, num_sms, st)
+                    : launch_bwd_mode<TW, TH, PPL, false>(a, batch, num_sms, st);
+}
+// 16x16 tiles: one warp per tile on large launches, two otherwise.
+cudaError_t launch_bwd_16(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
+  const uint32_t wave = (uint32_t)resident_per_sm<raster_bwd_tile_kernel<64, false>>(32) * (uint32_t)std::max(num_sms, 1);
+  if (a.vs.total_tiles >= kTileKernelWaves * wave || a.vs.total_tiles == 0)
     return a.ref_mode ? launch_bwd_tile16<true>(a, num_sms, st) : launch_bwd_tile16<false>(a, num_sms, st);
-  } else {
-    return a.ref_mode ? launch_bwd_mode<TW, TH, PPL, true>(a, batch, num_sms, st)
-                      : launch_bwd_mode<TW, TH, PPL, false>(a, batch, num_sms, st);
-  }
+  return launch_bwd_shape<16, 16, kBwdPPL16>(a, batch, num_sms, st);
 }
 
 }  // namespace
@@ -1255,7 +1278,8 @@ void raster_warm_up(uint32_t tile_w, uint32_t tile_h, uint32_t batch, int num_sm
     a.ref_mode = ref;
     if (tile_w == 16 && tile_h == 16) {
       (void)launch_fwd_shape<16, 16, kFwdPPL>(a, batch, num_sms, nullptr);
-      (void)launch_bwd_shape<16, 16, kBwdPPL>(a, batch, num_sms, nullptr);
+      (void)launch_bwd_16(a, batch, num_sms, nullptr);
+      (void)launch_bwd_shape<16, 16, kBwdPPL16>(a, batch, num_sms, nullptr);
     } else if (tile_w == 8 && tile_h == 8) {
       (void)launch_fwd_shape<8, 8, kFwdPPL>(a, batch, num_sms, nullptr);
       (void)launch_bwd_shape<8, 8, kBwdPPL>(a, batch, num_sms, nullptr);
@@ -1314,7 +1338,7 @@ cudaError_t launch_raster_bwd(const ViewSet& vs, FwdBufs& b, const float* bg, co
     cudaError_t e = cudaMemsetAsync(b.sched_ticket, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
   }
-  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_shape<16, 16, kBwdPPL>(a, vs.batch, s.num_sms, st);
+  if (vs.tile_w == 16 && vs.tile_h == 16) return launch_bwd_16(a, vs.batch, s.num_sms, st);
   if (vs.tile_w == 8 && vs.tile_h == 8) return launch_bwd_shape<8, 8, kBwdPPL>(a, vs.batch, s.num_sms, st);
   if (vs.tile_w == 32 && vs.tile_h == 8) return launch_bwd_shape<32, 8, kBwdPPL>(a, vs.batch, s.num_sms, st);
   return cudaErrorInvalidValue;
