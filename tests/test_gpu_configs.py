@@ -323,3 +323,43 @@ def test_more_tiles_than_emission_histograms_cover(gsr_ctx_factory, size, tile):
     for k in ("v_transforms", "v_sh", "v_raw_opacity"):
         assert_grad_parity(gg[k], ob[k], od[k], what=f"{w}x{h} {tile} {k}")
     ctx.close()
+
+
+@pytest.mark.parametrize("mode", ["exact", "reference"])
+def test_one_warp_tile_backward_modes(gsr_ctx_factory, mode):
+    """A 2560x1440 view has 14,400 16x16 tiles, more than four waves of the
+    one-warp-per-tile backward (16 CTAs per SM x 148 SMs x 4 = 9,472), so
+    the backward runs one warp per tile: both adjoints against the oracle
+    (screen-space sums, parameter gradients, statistics), and deterministic
+    mode bitwise equal across runs and within the parity bar of the default
+    reduction."""
+    import torch
+
+    from rustscan_b200 import host_splats_to_device
+
+    w, h = 2560, 1440
+    sc = S.config3(n=100_000, views=1, width=w, height=h, focal=1050.0 * w / 1280.0)
+    cam = sc.cameras[0]
+    up = S.upstream_grad(cam.height, cam.width)
+    m = 0 if mode == "exact" else 1
+    o = oracle_forward(sc, cam)
+    assert o.tiles_x * o.tiles_y >= 4 * 16 * 148
+    ob = o.backward(up, mode=m)
+    od = oracle_forward(sc, cam, f64=True).backward(up, mode=m)
+    splats = host_splats_to_device(sc)
+    runs = {}
+    for det in (False, True, True):
+        ctx = gsr_ctx_factory(max_splats=sc.n, max_pixels=w * h, max_isects=8 << 20, adjoint=mode, deterministic=det)
+        _, g = run_gpu_forward(ctx, splats, [cam])
+        assert_forward_parity(g[0], o)
+        gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(up, device="cuda"), stats=True))
+        torch.cuda.synchronize()
+        assert_grad_close(ctx.export(0, "splat_grads").reshape(-1, 12), ob["splat_grads"], rtol=1e-3,
+                          what=f"{mode} det={det} screen-space sums")
+        for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+            assert_grad_parity(gg[k], ob[k], od[k], what=f"{mode} det={det} {k}")
+        assert_grad_parity(gg["stats"][0], ob["stats"], od["stats"], what=f"{mode} det={det} stats")
+        runs.setdefault(det, []).append(gg)
+        ctx.close()
+    for k in ("v_transforms", "v_sh", "v_raw_opacity", "stats"):
+        np.testing.assert_array_equal(runs[True][0][k], runs[True][1][k], err_msg=k)
