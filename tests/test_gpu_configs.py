@@ -363,3 +363,37 @@ def test_one_warp_tile_backward_modes(gsr_ctx_factory, mode):
         ctx.close()
     for k in ("v_transforms", "v_sh", "v_raw_opacity", "stats"):
         np.testing.assert_array_equal(runs[True][0][k], runs[True][1][k], err_msg=k)
+
+
+def test_config5_batched_backward_against_one_view(gsr_ctx_factory):
+    """Config 5 as stated (2,000,000 Gaussians, 32 views of mixed resolution,
+    BF16 SH storage), backward of the whole batch in one launch per stage
+    with an upstream gradient on one 320x240 view and zeros on the other 31:
+    the parameter gradients equal that view's oracle adjoint (FP32 oracle fed
+    the stored SH, FP64 oracle beside it) within the parity bar."""
+    import torch
+
+    from oracle import oracle as O
+    from rustscan_b200 import host_splats_to_device
+
+    sc = S.config5()
+    cams = sc.cameras
+    pmax = max(c.width * c.height for c in cams)
+    sh_r = torch.as_tensor(sc.sh).to(torch.bfloat16).to(torch.float32).numpy()
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=len(cams), max_pixels=pmax, max_isects=24 << 20,
+                          sh_dtype="bf16")
+    splats = host_splats_to_device(sc, sh_dtype=torch.bfloat16)
+    _fit(ctx, splats, cams)
+    ctx.render_forward(splats, cams)
+    v = next(i for i, c in enumerate(cams) if (c.width, c.height) == (320, 240))
+    up_v = S.upstream_grad(cams[v].height, cams[v].width, seed=5)
+    ups = [up_v if i == v else np.zeros((c.height, c.width, 4), np.float32) for i, c in enumerate(cams)]
+    gg = _grads_np(ctx.render_backward(splats, torch.as_tensor(np.concatenate([u.reshape(-1) for u in ups]),
+                                                               device="cuda"), stats=False))
+    torch.cuda.synchronize()
+    ob = O.Forward(sc.transforms, sh_r, sc.raw_opacity, 3, cams[v]).backward(up_v, mode=0)
+    od = O.Forward(sc.transforms.astype(np.float64), sh_r.astype(np.float64), sc.raw_opacity.astype(np.float64), 3,
+                   cams[v], f64=True).backward(up_v.astype(np.float64), mode=0)
+    for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+        assert_grad_parity(gg[k], ob[k], od[k], what=f"config5 batched backward, view {v} {k}")
+    ctx.close()
