@@ -23,9 +23,9 @@ namespace {
 // their Gaussian with ballots, so each Gaussian's tiles keep their row-major
 // order and the output is the same as a per-Gaussian loop.
 struct WalkWarp {
-  uint32_t incl[32], ex[32];  // inclusive / exclusive prefix of box sizes
-  uint32_t x0[32], y0[32], w[32];
-  float mx[32], my[32], ca[32], cb[32], cc[32], thr[32];
+  uint4 box[32];      // exclusive prefix of box sizes, box width, box origin x, y
+  float4 g0[32];      // mean x, y, conic a, b
+  float4 g1[32];      // conic c, cut, 1 / box width, -
   uint32_t run[32];  // passing tiles found so far, per Gaussian
   uint32_t off[32];  // emission offset, per Gaussian
   uint32_t cid[32];  // compact index, per Gaussian
@@ -107,17 +107,9 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     __syncwarp();  // the previous round's readers of S are done
-    S.incl[lane] = incl;
-    S.ex[lane] = incl - nb;
-    S.x0[lane] = x0;
-    S.y0[lane] = y0;
-    S.w[lane] = w;
-    S.mx[lane] = mean.x;
-    S.my[lane] = mean.y;
-    S.ca[lane] = conic.x;
-    S.cb[lane] = conic.y;
-    S.cc[lane] = conic.z;
-    S.thr[lane] = thr;
+    S.box[lane] = make_uint4(incl - nb, w, x0, y0);
+    S.g0[lane] = make_float4(mean.x, mean.y, conic.x, conic.y);
+    S.g1[lane] = make_float4(conic.z, thr, w ? 1.0f / (float)w : 0.f, 0.f);
     S.run[lane] = 0u;
     S.off[lane] = o0;
     S.cid[lane] = c;
@@ -140,13 +132,31 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
       if (live) {
         const uint32_t upto = ((2u << lane) - 1u) & ~1u;  // positions 1..lane
         owner = S.lane_of_rank[r0 + (uint32_t)__popc(starts & upto)];
-        local = t - S.ex[owner];
-        const uint32_t ow = S.w[owner];
-        const uint32_t ry = local / ow;
-        tx = S.x0[owner] + (local - ry * ow);
-        ty = S.y0[owner] + ry;
-        pass = will_primitive_contribute(tx, ty, ts, V2<float>{S.mx[owner], S.my[owner]},
-                                         V3<float>{S.ca[owner], S.cb[owner], S.cc[owner]}, S.thr[owner]);
+        const uint4 bx = S.box[owner];
+        const float4 ga = S.g0[owner], gb = S.g1[owner];
+        local = t - bx.x;
+        // Row and column of the item in its box: the quotient from the
+        // float reciprocal is within one of the exact one for local < 2^24,
+        // and the remainder's range fixes it.
+        const uint32_t ow = bx.y;
+        uint32_t ry, rx;
+        if (local < (1u << 24)) {
+          ry = __float2uint_rz(__uint2float_rn(local) * gb.z);
+          rx = local - ry * ow;
+          if ((int32_t)rx < 0) {
+            --ry;
+            rx += ow;
+          } else if (rx >= ow) {
+            ++ry;
+            rx -= ow;
+          }
+        } else {
+          ry = local / ow;
+          rx = local - ry * ow;
+        }
+        tx = bx.z + rx;
+        ty = bx.w + ry;
+        pass = will_primitive_contribute(tx, ty, ts, V2<float>{ga.x, ga.y}, V3<float>{ga.z, ga.w, gb.x}, gb.y);
       }
       if (SLOTS) {
         if (live) {
@@ -408,10 +418,19 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
   cudaError_t e = cudaMemsetAsync(b.tile_hist, 0, sizeof(uint32_t) * b.Tcap * vs.n_views, st);
   if (e != cudaSuccess) return e;
   const size_t smem = sizeof(uint32_t) * vs.max_tiles;
-  if (slots)
+  // The per-tile counts may take the static walk state past the 48 KB
+  // default: allow the largest histogram.
+  if (slots) {
+    e = cudaFuncSetAttribute(tile_walk_kernel<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(uint32_t) * kHistMaxTiles));
+    if (e != cudaSuccess) return e;
     tile_walk_kernel<true, true, true><<<grid_for(vs, s.num_sms, kWalkBlocksPerSm), kWalkThreads, smem, st>>>(vs, b, 0);
-  else
+  } else {
+    e = cudaFuncSetAttribute(tile_walk_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(uint32_t) * kHistMaxTiles));
+    if (e != cudaSuccess) return e;
     tile_walk_kernel<true, true><<<grid_for(vs, s.num_sms, kWalkBlocksPerSm), kWalkThreads, smem, st>>>(vs, b, deterministic);
+  }
   return cudaGetLastError();
 }
 
