@@ -323,7 +323,7 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   // In the slot layout the tile sort drops the failing tiles' sentinel keys
   // in its first pass when its digits leave a spare digit value (below 8
   // bits), so the second pass and the scatter move real intersections only.
-  const bool drop_sentinels = b.slots && sort_digit_bits(tbits) < 8;
+  const bool drop_sentinels = b.slots && tile_first_digit_bits(tbits) < 8;
   if (tile_counts) {
     GSR_CUDA(c, launch_emit_hist(vs, b, c->s, c->cfg.deterministic, b.slots, st));
     GSR_CUDA(c, launch_tile_hist_finish(vs, b, c->s, tbits, b.slots, drop_sentinels, st));
@@ -335,11 +335,11 @@ gsr_status forward_impl(gsr_ctx* c, const gsr_splats* sp, const gsr_camera* cams
   if (b.pack_bits)
     GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, nullptr, b.isect_key, nullptr, b.key_tmp, nullptr, b.Icap, n_views,
                                  b.vcount + (b.slots ? 3 : 1), 4, 0, b.Icap, tbits, c->s, st, true, b.pack_bits,
-                                 real_counts));
+                                 real_counts, tile_first_digit_bits(tbits)));
   else
     GSR_CUDA(c, radix_sort_pairs(b.isect_key_raw, b.isect_val_raw, b.isect_key, b.isect_val, b.key_tmp, b.val_tmp,
                                  b.Icap, n_views, b.vcount + (b.slots ? 3 : 1), 4, 0, b.Icap, tbits, c->s, st,
-                                 tile_counts, 0, real_counts));
+                                 tile_counts, 0, real_counts, tile_counts ? tile_first_digit_bits(tbits) : 0));
   if (c->cfg.deterministic) GSR_CUDA(c, launch_remap(vs, b, c->s, st));
   prof_mark(c, kStRanges, st);
   if (!tile_counts) GSR_CUDA(c, launch_ranges(vs, b, c->s, st));

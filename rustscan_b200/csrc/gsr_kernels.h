@@ -122,11 +122,22 @@ inline int sort_digit_bits(int bits) {
   const int d = (bits + p - 1) / p;
   return d < 1 ? 1 : (d > 8 ? 8 : d);
 }
+// Digit widths of the tile sort (histograms from emission): the tile-id
+// digits of consecutive keys are spread in the low bits and clustered in the
+// high ones, so the second pass takes up to kTileSecondDigit bits and the
+// first the rest. Equal to sort_digit_bits for one pass.
+constexpr int kTileSecondDigit = 8;
+inline int tile_first_digit_bits(int bits) {
+  if (sort_passes(bits) != 2) return sort_digit_bits(bits);
+  const int d1 = kTileSecondDigit < bits - 1 ? kTileSecondDigit : bits - 1;
+  return bits - d1;
+}
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride,
                              uint32_t segments, const uint32_t* counts, uint32_t count_stride, uint32_t n_host,
                              uint64_t cap_per_segment, int bits, const Scratch& s, cudaStream_t st,
-                             bool hist_ready = false, uint32_t shift0 = 0, const uint32_t* counts_dropped = nullptr);
+                             bool hist_ready = false, uint32_t shift0 = 0, const uint32_t* counts_dropped = nullptr,
+                             int first_bits = 0);
 
 // Bounded-wait self-test: a look-back whose predecessor never publishes
 // (look-back states 0 and 1 are overwritten); gives up after max_polls.

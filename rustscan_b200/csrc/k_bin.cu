@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kWalkThreads) tile_walk_kernel(ViewSet vs, Fwd
 // tile id's digits, in the sort's histogram layout.
 constexpr int kHistThreads = 1024;
 __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet vs, FwdBufs b, uint32_t* hist,
-                                                                         uint32_t dbits, int slots) {
+                                                                         uint32_t dbits, uint32_t dbits1, int slots) {
   __shared__ uint32_t s_scan[32];
   __shared__ uint32_t s_h[2][256];
   const uint32_t v = blockIdx.x;
@@ -256,9 +256,8 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
       ranges[2 * t] = loc[i] ? run : 0u;
       ranges[2 * t + 1] = loc[i] ? run + loc[i] : 0u;
       if (loc[i]) {
-        const uint32_t dm = (1u << dbits) - 1u;
-        atomicAdd(&s_h[0][t & dm], loc[i]);
-        atomicAdd(&s_h[1][(t >> dbits) & dm], loc[i]);
+        atomicAdd(&s_h[0][t & ((1u << dbits) - 1u)], loc[i]);
+        atomicAdd(&s_h[1][(t >> dbits) & ((1u << dbits1) - 1u)], loc[i]);
       }
     }
     run += loc[i];
@@ -274,10 +273,9 @@ __global__ void __launch_bounds__(kHistThreads) tile_hist_finish_kernel(ViewSet 
     // dbits); over the sorted bits the key exceeds every tile id, so it
     // sorts last. The view's intersection count becomes the real one.
     const uint32_t written = b.vcount[v * 4 + 1];
-    const uint32_t dm = (1u << dbits) - 1u;
     if (slots == 1) {
-      atomicAdd(&s_h[0][(uint32_t)(0xffffffffull >> b.pack_bits) & dm], written - all);
-      atomicAdd(&s_h[1][(uint32_t)(0xffffffffull >> (b.pack_bits + dbits)) & dm], written - all);
+      atomicAdd(&s_h[0][(uint32_t)(0xffffffffull >> b.pack_bits) & ((1u << dbits) - 1u)], written - all);
+      atomicAdd(&s_h[1][(uint32_t)(0xffffffffull >> (b.pack_bits + dbits)) & ((1u << dbits1) - 1u)], written - all);
     }  // slots == 2: the sort drops the sentinels in its first pass
     b.vcount[v * 4 + 3] = written;
     b.vcount[v * 4 + 1] = all;
@@ -437,7 +435,9 @@ cudaError_t launch_emit_hist(const ViewSet& vs, FwdBufs& b, const Scratch& s, in
 cudaError_t launch_tile_hist_finish(const ViewSet& vs, FwdBufs& b, const Scratch& s, int tile_bits, bool slots,
                                    bool drop_sentinels, cudaStream_t st) {
   if (vs.max_tiles > kHistMaxTiles || sort_passes(tile_bits) > 2) return cudaErrorInvalidValue;
-  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)sort_digit_bits(tile_bits),
+  const int d0 = tile_first_digit_bits(tile_bits);
+  tile_hist_finish_kernel<<<vs.n_views, kHistThreads, 0, st>>>(vs, b, s.hist, (uint32_t)d0,
+                                                                (uint32_t)(tile_bits > d0 ? tile_bits - d0 : d0),
                                                                 slots ? (drop_sentinels ? 2 : 1) : 0);
   return cudaGetLastError();
 }

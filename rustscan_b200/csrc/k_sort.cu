@@ -317,12 +317,16 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint32_t* keys_tmp, uint32_t* vals_tmp, uint64_t seg_stride, uint32_t segments,
                              const uint32_t* counts, uint32_t count_stride, uint32_t n_host, uint64_t cap_per_segment,
                              int bits, const Scratch& s, cudaStream_t st, bool hist_ready, uint32_t shift0,
-                             const uint32_t* counts_dropped) {
+                             const uint32_t* counts_dropped, int first_bits) {
   if (segments == 0 || segments > (uint32_t)kMaxSegments) return cudaErrorInvalidValue;
   if (shift0 >= 32 || (keys_in == nullptr)) return cudaErrorInvalidValue;
   const bool kv = vals_out != nullptr;
-  const int dbits = sort_digit_bits(bits);
   const int passes = sort_passes(bits);
+  // Digit widths: uniform, or (with histograms from the caller and two
+  // passes) first_bits for the first pass and the rest for the second.
+  const bool split = first_bits > 0 && hist_ready && passes == 2 && first_bits < bits && bits - first_bits <= 8;
+  const int dbits = split ? first_bits : sort_digit_bits(bits);
+  auto pass_bits = [&](int p) { return split ? (p == 0 ? first_bits : bits - first_bits) : dbits; };
   // Dropping the all-ones keys in the first pass needs a spare digit value.
   const bool drop = counts_dropped != nullptr;
   if (drop && (dbits >= 8 || !hist_ready)) return cudaErrorInvalidValue;
@@ -354,8 +358,8 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     a.drop = (drop && p == 0) ? 1u : 0u;
     a.n_host = n_host;
     a.cap = cap_per_segment;
-    a.shift = shift0 + dbits * p;
-    a.dmask = (1u << dbits) - 1u;
+    a.shift = shift0 + dbits * p;  // a split's second pass starts after the first's bits
+    a.dmask = (1u << pass_bits(p)) - 1u;
     a.pass = p;
     a.base = s.hist_base;
     a.states = s.lb_states;
