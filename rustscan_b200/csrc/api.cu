@@ -157,7 +157,7 @@ gsr_status allocate(gsr_ctx* c) {
             dalloc(c, &b.tile_hist, nv * T) && dalloc(c, &b.hitw, nv * I) && dalloc(c, &b.sched_order, nv * T) &&
             dalloc(c, &b.sched_lists, 33 * nv * T) && dalloc(c, &b.sched_lcount, 33) && dalloc(c, &b.sched_ticket, 1);
   b.sched_items_cap = nv * T;
-  b.proj_parts_cap = (uint32_t)((N + 255) / 256);
+  b.proj_parts_cap = (uint32_t)((N + kProjBlock - 1) / kProjBlock);
   ok = ok && dalloc(c, &b.vis_bits, nv * b.proj_parts_cap * 8) && dalloc(c, &b.blk_count, nv * b.proj_parts_cap) &&
        dalloc(c, &b.blk_base, nv * b.proj_parts_cap);
   if (ok && cfg.deterministic)

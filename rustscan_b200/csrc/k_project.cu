@@ -27,7 +27,7 @@ namespace gsr {
 
 namespace {
 
-constexpr int kProjThreads = 256;
+constexpr int kProjThreads = (int)kProjBlock;
 
 struct ProjectArgs {
   SplatsDev sp;
@@ -187,8 +187,8 @@ __global__ void __launch_bounds__(kProjThreads) records_kernel(ProjectArgs a) {
   const uint32_t rows = min(n - g0, (uint32_t)kProjThreads);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   sh_rows_issue<DEG>(reinterpret_cast<const SHT*>(a.sp.sh), g0, rows, s_sh);
-  if (threadIdx.x < nv * kWarps) {
-    const uint32_t v = threadIdx.x / kWarps, w = threadIdx.x % kWarps;
+  for (uint32_t i = threadIdx.x; i < nv * kWarps; i += kProjThreads) {
+    const uint32_t v = i / kWarps, w = i % kWarps;
     s_mask[v][w] = a.vis_bits[(size_t)v * a.words + part * kWarps + w];
   }
   if (threadIdx.x < nv) s_base[threadIdx.x] = a.blk_base[(size_t)threadIdx.x * a.parts + part];
