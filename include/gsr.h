@@ -302,6 +302,19 @@ GSR_API gsr_status gsr_train_step(gsr_ctx* ctx, float* transforms, void* sh, flo
                           const float* targets, const gsr_train_params* params, float* densify_acc, float* loss,
                           int32_t use_graph, void* stream);
 
+/* gsr_train_step whose loss waits on targets_ready (a cudaEvent_t, or NULL
+ * for no wait): the forward is launched first and the stream waits on the
+ * event's latest record before the loss reads targets, so that the targets'
+ * upload and conversion on another stream overlap the forward (the
+ * reference uploads them before its forward, engine/trainer.rs:265-268).
+ * With use_graph != 0 and an event, the forward and the rest are recorded
+ * as two graphs with the wait between their launches. */
+GSR_API gsr_status gsr_train_step_after(gsr_ctx* ctx, float* transforms, void* sh, float* raw_opacity, uint32_t n,
+                                uint32_t sh_degree, const gsr_adam_state* state, const gsr_camera* cams,
+                                uint32_t n_views, const float* targets, const gsr_train_params* params,
+                                float* densify_acc, float* loss, int32_t use_graph, void* targets_ready,
+                                void* stream);
+
 /* ---- topology (RustGS/src/training/topology/apply.rs) -------------------- */
 /* A topology plan row: the output splat copies splat `source`, as is
  * (GSR_TOPO_EXISTING) or as one half of a split, moved by -offset

@@ -575,7 +575,11 @@ class Trainer:
         self._frames = None  # 8-bit frame pipeline: the same, with a byte staging buffer
         self._frames_prefetched = None
 
-    def train_step(self, cameras, targets: torch.Tensor, iteration: int):
+    def train_step(self, cameras, targets: torch.Tensor, iteration: int, targets_ready=None):
+        """One training step on the current stream (gsr_train_step). With
+        targets_ready (a torch.cuda.Event recorded after the work that writes
+        targets), the forward is launched at once and the loss waits on the
+        event (gsr_train_step_after). Returns the per-view losses (device)."""
         cams = list(cameras)
         if self.loss is None or self.loss.numel() != len(cams):
             self.loss = torch.zeros(len(cams), dtype=torch.float32, device="cuda")
@@ -591,10 +595,13 @@ class Trainer:
             self._cams = cams
         st = self.opt.state()
         s = self.splats
-        self.ctx._check(self.ctx._lib.gsr_train_step(
-            self.ctx._h, _ptr(s.transforms), _ptr(s.sh_coeffs), _ptr(s.raw_opacities), s.num_splats(), s.sh_degree,
-            C.byref(st), self._arr, len(cams), _ptr(targets), C.byref(p), _ptr(self.densify), _ptr(self.loss),
-            int(self.use_graph), _stream()))
+        args = (self.ctx._h, _ptr(s.transforms), _ptr(s.sh_coeffs), _ptr(s.raw_opacities), s.num_splats(), s.sh_degree,
+                C.byref(st), self._arr, len(cams), _ptr(targets), C.byref(p), _ptr(self.densify), _ptr(self.loss),
+                int(self.use_graph))
+        if targets_ready is None:
+            self.ctx._check(self.ctx._lib.gsr_train_step(*args, _stream()))
+        else:
+            self.ctx._check(self.ctx._lib.gsr_train_step_after(*args, C.c_void_p(targets_ready.cuda_event), _stream()))
         return self.loss
 
     def train_step_frames(self, cameras, frames, iteration: int, next_frames=None):
@@ -602,13 +609,14 @@ class Trainer:
         memory (frames: one [H,W,3] uint8 tensor per camera, e.g.
         frames.DecodedFrame.rgb).
 
-        The bytes (a quarter of the f32 volume) cross to the device, or were
-        already copied there on a side stream during the previous call when
-        that call was given them as next_frames; gsr_frames_to_targets then
-        converts them into the step's target buffer (resizing frames whose
-        size differs from the camera's), and the step runs on the current
-        stream. next_frames, if given, start copying while this step runs.
-        Returns the per-view losses (device)."""
+        On a side stream the bytes (a quarter of the f32 volume) cross to the
+        device, unless the previous call was given them as next_frames and
+        copied them already, and gsr_frames_to_targets converts them into the
+        step's target buffer (resizing frames whose size differs from the
+        camera's). Meanwhile the step's forward runs on the current stream;
+        its loss waits for the targets (gsr_train_step_after). next_frames,
+        if given, start copying while this step runs. Returns the per-view
+        losses (device)."""
         cams = list(cameras)
         frames = list(frames)
         if len(frames) != len(cams):
@@ -616,35 +624,6 @@ class Trainer:
         for f in frames:
             if f.dtype != torch.uint8 or f.dim() != 3 or f.shape[2] != 3 or not f.is_pinned():
                 raise ValueError("frames must be pinned [H,W,3] uint8 tensors")
-        sizes = [f.numel() for f in frames]
-        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).tolist()
-        descs = [(o, f.shape[1], f.shape[0]) for o, f in zip(offs, frames)]
-        n_t = sum(c.width * c.height * 3 for c in cams)
-        main = torch.cuda.current_stream()
-        h = self._frames
-        if h is None or h["stage"].numel() < sum(sizes) or h["dev"].numel() != n_t:
-            h = self._frames = {
-                "dev": torch.empty(n_t, dtype=torch.float32, device="cuda"),
-                "stage": torch.empty(max(sum(sizes), 1), dtype=torch.uint8, device="cuda"),
-                "stream": torch.cuda.Stream(),
-                "ready": torch.cuda.Event(),
-                "free": torch.cuda.Event(),
-            }
-            self._frames_prefetched = None
-
-        def upload(src):
-            for f, o, nb in zip(src, offs, sizes):
-                h["stage"][o:o + nb].copy_(f.reshape(-1), non_blocking=True)
-
-        pre = self._frames_prefetched
-        if pre is not None and len(pre) == len(frames) and all(a is b for a, b in zip(pre, frames)):
-            main.wait_event(h["ready"])
-        else:
-            upload(frames)
-        self.ctx.frames_to_targets(h["stage"], descs, cams, out=h["dev"])
-        h["free"].record(main)  # the staging bytes have been read
-        loss = self.train_step(cams, h["dev"], iteration)
-        self._frames_prefetched = None
         if next_frames is not None:
             nxt = list(next_frames)
             if [tuple(f.shape) for f in nxt] != [tuple(f.shape) for f in frames]:
@@ -652,11 +631,46 @@ class Trainer:
             for f in nxt:
                 if f.dtype != torch.uint8 or not f.is_pinned():
                     raise ValueError("frames must be pinned [H,W,3] uint8 tensors")
-            cs = h["stream"]
-            cs.wait_event(h["free"])
+        sizes = [f.numel() for f in frames]
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).tolist()
+        descs = [(o, f.shape[1], f.shape[0]) for o, f in zip(offs, frames)]
+        n_t = sum(c.width * c.height * 3 for c in cams)
+        main = torch.cuda.current_stream()
+        h = self._frames
+        if h is None or h["stage"].numel() < sum(sizes) or h["dev"].numel() != n_t:
+            if h is not None:
+                main.wait_stream(h["stream"])  # the old buffers are freed in main's order: no reuse under a copy
+            h = self._frames = {
+                "dev": torch.empty(n_t, dtype=torch.float32, device="cuda"),
+                "stage": torch.empty(max(sum(sizes), 1), dtype=torch.uint8, device="cuda"),
+                "stream": torch.cuda.Stream(),
+                "ready": torch.cuda.Event(),
+                "dev_free": torch.cuda.Event(),
+            }
+            self._frames_prefetched = None
+            h["stream"].wait_stream(main)  # the new buffers' allocation is ordered before their use
+
+        def upload(src):
+            for f, o, nb in zip(src, offs, sizes):
+                h["stage"][o:o + nb].copy_(f.reshape(-1), non_blocking=True)
+
+        cs = h["stream"]
+        pre = self._frames_prefetched
+        with torch.cuda.stream(cs):
+            # Stream order on cs puts the copy after the previous conversion
+            # (the last reader of the staging bytes); the conversion waits
+            # until the previous step's loss has read the target buffer.
+            if not (pre is not None and len(pre) == len(frames) and all(a is b for a, b in zip(pre, frames))):
+                upload(frames)
+            cs.wait_event(h["dev_free"])
+            self.ctx.frames_to_targets(h["stage"], descs, cams, out=h["dev"])
+            h["ready"].record(cs)
+        loss = self.train_step(cams, h["dev"], iteration, targets_ready=h["ready"])
+        h["dev_free"].record(main)
+        self._frames_prefetched = None
+        if next_frames is not None:
             with torch.cuda.stream(cs):
                 upload(nxt)
-            h["ready"].record(cs)
             self._frames_prefetched = nxt  # held, so the identity check above stays sound
         return loss
 

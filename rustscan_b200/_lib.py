@@ -161,6 +161,7 @@ EXPORTED = [
     "gsr_adam_step",
     "gsr_accumulate_densify",
     "gsr_train_step",
+    "gsr_train_step_after",
     "gsr_profile",
     "gsr_profile_read",
     "gsr_graph_kernel_count",
@@ -211,6 +212,8 @@ def load():
     L.gsr_accumulate_densify.argtypes = [vp, C.POINTER(gsr_grads), vp, vp, u32, u32, i32, vp, vp]
     L.gsr_train_step.argtypes = [vp, vp, vp, vp, u32, u32, C.POINTER(gsr_adam_state), C.POINTER(gsr_camera), u32,
                                  vp, C.POINTER(gsr_train_params), vp, vp, i32, vp]
+    L.gsr_train_step_after.argtypes = [vp, vp, vp, vp, u32, u32, C.POINTER(gsr_adam_state), C.POINTER(gsr_camera),
+                                       u32, vp, C.POINTER(gsr_train_params), vp, vp, i32, vp, vp]
     L.gsr_profile.argtypes = [vp, i32]
     L.gsr_profile_read.argtypes = [vp, C.POINTER(C.c_float), i32, vp]
     L.gsr_graph_kernel_count.argtypes = [vp]

@@ -56,8 +56,11 @@ struct gsr_ctx {
   float* grad_work = nullptr;  // summed gradient of a training step: [N][10], [N][3K<=75], [N] (16-byte aligned)
   uint64_t grad_sh_off = 0, grad_op_off = 0;
   AdamScalars* d_scal = nullptr;
-  // graph cache of the training step
+  // graph cache of the training step: the whole step, or (when the step
+  // waits on a targets-ready event) its forward here and the rest in
+  // graph_exec_rest
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph_exec_rest = nullptr;
   std::vector<uint8_t> graph_key;
   int graph_kernels = 0;
   cudaStream_t capture_stream = nullptr;  // graphs are recorded here (the legacy default stream cannot capture)
@@ -128,6 +131,8 @@ void free_all(gsr_ctx* c) {
   c->allocs.clear();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   c->graph_exec = nullptr;
+  if (c->graph_exec_rest) cudaGraphExecDestroy(c->graph_exec_rest);
+  c->graph_exec_rest = nullptr;
   if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
   c->capture_stream = nullptr;
 }
@@ -671,16 +676,15 @@ gsr_status gsr_accumulate_densify(gsr_ctx* c, const gsr_grads* g, const float* s
   return GSR_OK;
 }
 
-static gsr_status train_body(gsr_ctx* c, const gsr_splats* sp, float* transforms, void* sh, float* raw_opacity,
-                             const gsr_adam_state* state, const gsr_camera* cams, uint32_t n_views,
-                             const float* targets, const gsr_train_params* p, float* densify_acc, float* loss,
-                             cudaStream_t st) {
-  gsr_status rs = forward_impl(c, sp, cams, n_views, c->render, nullptr, st);
-  if (rs != GSR_OK) return rs;
+// The step after its forward: loss, raster backward, projection backward
+// with the densification statistics, Adam.
+static gsr_status train_rest(gsr_ctx* c, const gsr_splats* sp, float* transforms, void* sh, float* raw_opacity,
+                             const gsr_adam_state* state, uint32_t n_views, const float* targets,
+                             const gsr_train_params* p, float* densify_acc, float* loss, cudaStream_t st) {
   prof_mark(c, kStLoss, st);
   GSR_CUDA(c, launch_loss(c->fwd_vs, c->fwd_desc.data(), c->render, targets, p->l1_weight, p->ssim_weight, loss,
                           c->v_render, c->loss_work, c->loss_work_floats, st));
-  rs = raster_backward_impl(c, c->v_render, st);
+  const gsr_status rs = raster_backward_impl(c, c->v_render, st);
   if (rs != GSR_OK) return rs;
   AdamArgs a{};
   a.transforms = transforms;
@@ -711,17 +715,61 @@ static gsr_status train_body(gsr_ctx* c, const gsr_splats* sp, float* transforms
   return GSR_OK;
 }
 
-gsr_status gsr_train_step(gsr_ctx* c, float* transforms, void* sh, float* raw_opacity, uint32_t n, uint32_t sh_degree,
-                          const gsr_adam_state* state, const gsr_camera* cams, uint32_t n_views, const float* targets,
-                          const gsr_train_params* p, float* densify_acc, float* loss, int32_t use_graph,
-                          void* stream) {
+// Captures what `body` launches on the capture stream into an executable
+// graph and adds its kernel nodes to c->graph_kernels.
+extern "C++" template <class Body>
+gsr_status capture_graph(gsr_ctx* c, Body body, cudaGraphExec_t* out) {
+  if (!c->capture_stream) GSR_CUDA(c, cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
+  cudaStream_t cs = c->capture_stream;
+  cudaGraph_t graph = nullptr;
+  GSR_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  gsr_status rs = body(cs);
+  cudaError_t e = cudaStreamEndCapture(cs, &graph);
+  if (rs != GSR_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rs;
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  size_t nn = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+      for (size_t i = 0; i < nn; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++c->graph_kernels;
+      }
+  }
+  e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return cuda_fail(c, e, "cudaGraphInstantiate");
+  }
+  return GSR_OK;
+}
+
+static gsr_status train_step_impl(gsr_ctx* c, float* transforms, void* sh, float* raw_opacity, uint32_t n,
+                                  uint32_t sh_degree, const gsr_adam_state* state, const gsr_camera* cams,
+                                  uint32_t n_views, const float* targets, const gsr_train_params* p,
+                                  float* densify_acc, float* loss, int32_t use_graph, cudaEvent_t ready,
+                                  cudaStream_t st) {
   if (!c) return GSR_ERR_INVALID_ARG;
   if (!state || !p || !targets || !loss || p->step < 1) return fail(c, GSR_ERR_INVALID_ARG, "bad training arguments");
-  cudaStream_t st = (cudaStream_t)stream;
   gsr_splats sp{transforms, sh, raw_opacity, n, sh_degree};
   GSR_CUDA(c, launch_set_scalars(c->d_scal, make_scalars(&p->lr, p->step), st));
-  if (!use_graph) return train_body(c, &sp, transforms, sh, raw_opacity, state, cams, n_views, targets, p, densify_acc, loss, st);
-  // Graph key: everything baked into the captured launches.
+  auto fwd = [&](cudaStream_t s) { return forward_impl(c, &sp, cams, n_views, c->render, nullptr, s); };
+  auto rest = [&](cudaStream_t s) {
+    return train_rest(c, &sp, transforms, sh, raw_opacity, state, n_views, targets, p, densify_acc, loss, s);
+  };
+  if (!use_graph) {
+    gsr_status rs = fwd(st);
+    if (rs != GSR_OK) return rs;
+    if (ready) GSR_CUDA(c, cudaStreamWaitEvent(st, ready, 0));
+    return rest(st);
+  }
+  // Graph key: everything baked into the captured launches, and whether the
+  // step is split at the event wait.
+  const uint8_t split = ready != nullptr;
   std::vector<uint8_t> key;
   auto put = [&](const void* d, size_t sz) {
     const uint8_t* q = static_cast<const uint8_t*>(d);
@@ -741,46 +789,64 @@ gsr_status gsr_train_step(gsr_ctx* c, float* transforms, void* sh, float* raw_op
   put(&p->l1_weight, 4);
   put(&p->ssim_weight, 4);
   put(&p->use_visible, 4);
+  put(&split, 1);
   if (c->graph_exec == nullptr || key != c->graph_key) {
-    if (c->graph_exec) {
-      cudaGraphExecDestroy(c->graph_exec);
-      c->graph_exec = nullptr;
-    }
+    for (cudaGraphExec_t* g : {&c->graph_exec, &c->graph_exec_rest})
+      if (*g) {
+        cudaGraphExecDestroy(*g);
+        *g = nullptr;
+      }
+    c->graph_key.clear();
     std::vector<ViewDesc> desc;
     ViewSet vs;
     gsr_status rs = build_views(c, cams, n_views, desc, vs);
     if (rs != GSR_OK) return rs;
-    cudaGraph_t graph = nullptr;
-    if (!c->capture_stream) GSR_CUDA(c, cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
-    cudaStream_t cs = c->capture_stream;
-    GSR_CUDA(c, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    rs = train_body(c, &sp, transforms, sh, raw_opacity, state, cams, n_views, targets, p, densify_acc, loss, cs);
-    cudaError_t e = cudaStreamEndCapture(cs, &graph);
-    if (rs != GSR_OK) {
-      if (graph) cudaGraphDestroy(graph);
-      return rs;
-    }
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
-    size_t nn = 0;
     c->graph_kernels = 0;
-    if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
-      std::vector<cudaGraphNode_t> nodes(nn);
-      if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
-        for (size_t i = 0; i < nn; ++i) {
-          cudaGraphNodeType t;
-          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++c->graph_kernels;
-        }
+    if (split) {
+      rs = capture_graph(c, fwd, &c->graph_exec);
+      if (rs == GSR_OK) rs = capture_graph(c, rest, &c->graph_exec_rest);
+    } else {
+      rs = capture_graph(
+          c,
+          [&](cudaStream_t s) {
+            gsr_status r = fwd(s);
+            return r != GSR_OK ? r : rest(s);
+          },
+          &c->graph_exec);
     }
-    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      c->graph_exec = nullptr;
-      return cuda_fail(c, e, "cudaGraphInstantiate");
+    if (rs != GSR_OK) {
+      for (cudaGraphExec_t* g : {&c->graph_exec, &c->graph_exec_rest})
+        if (*g) {
+          cudaGraphExecDestroy(*g);
+          *g = nullptr;
+        }
+      return rs;
     }
     c->graph_key = key;
   }
   GSR_CUDA(c, cudaGraphLaunch(c->graph_exec, st));
+  if (split) {
+    GSR_CUDA(c, cudaStreamWaitEvent(st, ready, 0));
+    GSR_CUDA(c, cudaGraphLaunch(c->graph_exec_rest, st));
+  }
   return GSR_OK;
+}
+
+gsr_status gsr_train_step(gsr_ctx* c, float* transforms, void* sh, float* raw_opacity, uint32_t n, uint32_t sh_degree,
+                          const gsr_adam_state* state, const gsr_camera* cams, uint32_t n_views, const float* targets,
+                          const gsr_train_params* p, float* densify_acc, float* loss, int32_t use_graph,
+                          void* stream) {
+  return train_step_impl(c, transforms, sh, raw_opacity, n, sh_degree, state, cams, n_views, targets, p, densify_acc,
+                         loss, use_graph, nullptr, (cudaStream_t)stream);
+}
+
+gsr_status gsr_train_step_after(gsr_ctx* c, float* transforms, void* sh, float* raw_opacity, uint32_t n,
+                                uint32_t sh_degree, const gsr_adam_state* state, const gsr_camera* cams,
+                                uint32_t n_views, const float* targets, const gsr_train_params* p,
+                                float* densify_acc, float* loss, int32_t use_graph, void* targets_ready,
+                                void* stream) {
+  return train_step_impl(c, transforms, sh, raw_opacity, n, sh_degree, state, cams, n_views, targets, p, densify_acc,
+                         loss, use_graph, (cudaEvent_t)targets_ready, (cudaStream_t)stream);
 }
 
 gsr_status gsr_profile(gsr_ctx* c, int32_t enable) {

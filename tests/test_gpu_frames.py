@@ -53,10 +53,12 @@ def test_frames_to_targets_rejects_bad_input(gsr_ctx_factory):
     assert ei.value.status == 1
 
 
-def test_frame_fed_step_equals_oracle_targets(gsr_ctx_factory):
-    """Trainer.train_step_frames (bytes prefetched on a side stream, converted
-    on the device) is bit-identical to train_step on the oracle's f32
-    targets of the same frames, over a sequence that changes frames and
+@pytest.mark.parametrize("prefetch", [True, False])
+def test_frame_fed_step_equals_oracle_targets(gsr_ctx_factory, prefetch):
+    """Trainer.train_step_frames (bytes copied on a side stream, prefetched
+    by the step before or copied by the step itself, converted on the device
+    while the forward runs) is bit-identical to train_step on the oracle's
+    f32 targets of the same frames, over a sequence that changes frames and
     resizes one view."""
     import torch
 
@@ -75,7 +77,7 @@ def test_frame_fed_step_equals_oracle_targets(gsr_ctx_factory):
     ta = Trainer(ctx_a, sa, lrs, use_graph=True, total_iterations=100)
     tb = Trainer(ctx_b, sb, lrs, use_graph=True, total_iterations=100)
     for it, k in enumerate(order, start=1):
-        nxt = host[order[it]] if it < len(order) else None
+        nxt = host[order[it]] if prefetch and it < len(order) else None
         la = ta.train_step_frames(sc.cameras, host[k], it, next_frames=nxt).clone()
         tgt = np.concatenate([O.frame_to_target(f, w, h, 64, 48).reshape(-1) for f, (w, h) in zip(seqs[k], src_sizes)])
         lb = tb.train_step(sc.cameras, torch.as_tensor(tgt, device="cuda"), it).clone()

@@ -102,6 +102,48 @@ def test_train_step_equals_unfused_composition(gsr_ctx_factory, use_graph):
         np.testing.assert_array_equal(sa.raw_opacities.cpu().numpy(), sb.raw_opacities.cpu().numpy())
 
 
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_train_step_after_event_equals_plain_step(gsr_ctx_factory, use_graph):
+    """gsr_train_step_after (the forward launched first, the loss waiting on
+    a targets-ready event; with graphs, two graphs with the wait between
+    them) is bit-identical to gsr_train_step, and its graphs hold the same
+    kernels. The targets are written on a side stream before the event."""
+    import torch
+
+    from rustscan_b200 import LearningRates, Trainer
+
+    sc, targets = _scene_pair()
+    nv = len(sc.cameras)
+    tgt = torch.as_tensor(np.concatenate([t.reshape(-1) for t in targets]), device="cuda")
+    lrs = LearningRates()
+    ctx_a = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48, deterministic=True)
+    ctx_b = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48, deterministic=True)
+    sa, sb = _dev(sc), _dev(sc)
+    ta = Trainer(ctx_a, sa, lrs, use_graph=use_graph, total_iterations=100)
+    tb = Trainer(ctx_b, sb, lrs, use_graph=use_graph, total_iterations=100)
+    side = torch.cuda.Stream()
+    ready, done = torch.cuda.Event(), torch.cuda.Event()
+    tgt_b = torch.zeros_like(tgt)
+    side.wait_stream(torch.cuda.current_stream())
+    for it in range(1, 5):
+        la = ta.train_step(sc.cameras, tgt, it).clone()
+        with torch.cuda.stream(side):
+            side.wait_event(done)  # the previous step's loss has read tgt_b
+            tgt_b.copy_(tgt * 1.0)
+            ready.record(side)
+        lb = tb.train_step(sc.cameras, tgt_b, it, targets_ready=ready).clone()
+        done.record(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(la.cpu().numpy(), lb.cpu().numpy())
+        np.testing.assert_array_equal(sa.transforms.cpu().numpy(), sb.transforms.cpu().numpy())
+        np.testing.assert_array_equal(sa.sh_coeffs.cpu().numpy(), sb.sh_coeffs.cpu().numpy())
+        np.testing.assert_array_equal(sa.raw_opacities.cpu().numpy(), sb.raw_opacities.cpu().numpy())
+    if use_graph:
+        ka = int(ctx_a._lib.gsr_graph_kernel_count(ctx_a._h))
+        kb = int(ctx_b._lib.gsr_graph_kernel_count(ctx_b._h))
+        assert ka == kb and ka > 0, (ka, kb)
+
+
 def test_train_step_loss_and_statistics_vs_oracle(gsr_ctx_factory):
     """First step: per-view losses and the densification statistics agree with
     the oracle composition (loss -> exact adjoint -> trainer.rs:651-728)."""
