@@ -193,6 +193,7 @@ GSR_API gsr_status gsr_render_forward(gsr_ctx* ctx, const gsr_splats* splats, co
  * layout as out_rgba). Writes the parameter gradients of the sum over views
  * (rows of Gaussians no view sees are zero) and, if stats is not NULL, the
  * [n_views, n, 7] densification statistics (project_backwards.wgsl:33-36, 105-108).
+ * With n == 0 the gradient arrays are empty and may be NULL.
  * Replaces RenderBackward::backward (RustGS/src/training/backward/autodiff.rs:82-142)
  * and, below it, RasterizeBwdBackend (rasterize_bwd.rs:41-54) and
  * ProjectBwdBackend (project_bwd.rs:44-52). */

@@ -511,7 +511,8 @@ gsr_status gsr_render_backward(gsr_ctx* c, const gsr_splats* sp, const float* v_
   if (rs != GSR_OK) return rs;
   if (sp->n != c->fwd_n || (int)sp->sh_degree != c->fwd_degree)
     return fail(c, GSR_ERR_INVALID_ARG, "splats differ from the last forward");
-  if (!v_rgba || !grads || !grads->v_transforms || !grads->v_sh || !grads->v_raw_opacity)
+  // With no Gaussians the gradient arrays are empty and may be null.
+  if (!v_rgba || !grads || (sp->n > 0 && (!grads->v_transforms || !grads->v_sh || !grads->v_raw_opacity)))
     return fail(c, GSR_ERR_INVALID_ARG, "null gradient buffer");
   cudaStream_t st = (cudaStream_t)stream;
   rs = raster_backward_impl(c, v_rgba, st);

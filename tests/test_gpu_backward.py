@@ -123,3 +123,45 @@ def test_single_splat_backward_known_answer(gsr_ctx_factory):
     assert s[11] > 0
     ob = oracle_forward(sc, cam).backward(up, mode=0)
     assert_grad_close(g["splat_grads"][0], ob["splat_grads"], rtol=1e-3, what="single splat")
+
+
+def test_backward_edge_cases(gsr_ctx_factory):
+    """The forward's edge scenes through the backward: no Gaussian at all,
+    only culled ones (behind the camera, zero quaternion, off screen,
+    transparent), one covering the whole image, a single small one and all
+    of them together; parameter gradients and statistics against the oracle
+    (rows of culled Gaussians zero)."""
+    cam = S.camera_from_rt(np.eye(3), np.array([0.0, 0.0, 3.0]), 64, 64, 32, 32, 64, 64)
+    rows = []
+
+    def g(pos, ls, q=(1, 0, 0, 0), op=2.0, rgb=(0.9, 0.2, 0.1)):
+        tr = np.zeros(10, np.float32)
+        tr[0:3] = pos
+        tr[3:7] = q
+        tr[7:10] = ls
+        rows.append((tr, ((np.asarray(rgb) - 0.5) / S.SH_C0).reshape(1, 3), op))
+
+    g((0, 0, -5), (-2, -2, -2))            # behind the camera
+    g((0, 0, 0), (0.5, 0.5, 0.5))          # covers the image
+    g((0.1, 0.1, 0.5), (-3, -3, -3), q=(0, 0, 0, 0))  # zero quaternion: culled
+    g((0.3, -0.2, 0.2), (-3, -2.5, -4))
+    g((5, 5, 0), (-3, -3, -3))             # off screen
+    g((0.0, 0.0, 0.0), (-3, -3, -3), op=-8.0)  # transparent: culled
+    tr = np.stack([r[0] for r in rows])
+    sh = np.stack([r[1] for r in rows]).astype(np.float32)
+    op = np.asarray([r[2] for r in rows], np.float32)
+    up = S.upstream_grad(64, 64, seed=41)
+    for sel in ([], [0, 2, 4, 5], [1], [3], [0, 1, 2, 3, 4, 5]):
+        sc = S.Scene(tr[sel].reshape(-1, 10), sh[sel].reshape(-1, 1, 3), op[sel].reshape(-1), 0, [cam])
+        ctx = gsr_ctx_factory(max_splats=8, max_pixels=64 * 64)
+        splats = _dev(sc)
+        run_gpu_forward(ctx, splats, [cam])
+        gg = _backward(ctx, splats, [cam], [up])
+        if not sel:
+            assert gg["v_transforms"].shape == (0, 10) and gg["v_raw_opacity"].shape == (0,)
+            continue
+        ob = oracle_forward(sc, cam).backward(up, mode=0)
+        od = oracle_forward(sc, cam, f64=True).backward(up, mode=0)
+        for k in ("v_transforms", "v_sh", "v_raw_opacity"):
+            assert_grad_parity(gg[k], ob[k], od[k], what=f"{sel} {k}")
+        assert_grad_parity(gg["stats"][0], ob["stats"], od["stats"], what=f"{sel} stats")

@@ -168,6 +168,63 @@ def test_train_step_loss_and_statistics_vs_oracle(gsr_ctx_factory):
     assert_grad_close(tr.densify.cpu().numpy(), acc, rtol=1e-3, what="densification statistics")
 
 
+def test_train_step_with_empty_and_ragged_views(gsr_ctx_factory):
+    """A batch holding a view that sees no Gaussian (the camera looks away
+    from the scene) and a view whose size is a multiple of neither the tile
+    nor the SSIM tile: per-view losses and densification statistics of the
+    training step agree with the oracle, and the batch's gradients from the
+    separate entry points equal the sum of the per-view oracle adjoints."""
+    import torch
+
+    from _parity import assert_grad_parity
+    from rustscan_b200 import LearningRates, Trainer
+
+    sc, _ = _scene_pair(seed=84)
+    gt, _ = _scene_pair(seed=85)
+    f = 0.9 * 50
+    away = S.look_at(np.array([0.0, 0.0, 6.0]), (0.0, 0.0, 10.0), 0.9 * 64, 0.9 * 64, 31.75, 24.5, 64, 48)
+    ragged = S.look_at(np.array([2.0, 1.5, 2.4]), (0.0, 0.0, 0.0), f, f * 1.05, 24.75, 19.0, 50, 37)
+    cams = [sc.cameras[0], away, ragged]
+    sc.cameras = cams
+    gt.cameras = cams
+    targets = [oracle_forward(gt, cam).image[..., :3].copy() for cam in cams]
+    fwd = [oracle_forward(sc, cam) for cam in cams]
+    assert fwd[1].num_visible == 0 and fwd[0].num_visible > 0 and fwd[2].num_visible > 0
+    tgt = torch.as_tensor(np.concatenate([t.reshape(-1) for t in targets]), device="cuda")
+    nv = len(cams)
+
+    ctx = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48)
+    splats = _dev(sc)
+    tr = Trainer(ctx, splats, LearningRates(), use_graph=True)
+    loss = tr.train_step(cams, tgt, 1).cpu().numpy()
+    acc = np.zeros((9, sc.n), np.float32)
+    keys = ("v_transforms", "v_sh", "v_raw_opacity")
+    r32 = {k: 0.0 for k in keys}
+    r64 = {k: 0.0 for k in keys}
+    vps = []
+    for v, cam in enumerate(cams):
+        lv, vp = O.loss(fwd[v].image, targets[v])
+        vps.append(vp)
+        # The empty view renders the background against a background target:
+        # its loss is a few ulps of SSIM's 1 at most, hence the absolute term.
+        assert abs(loss[v] - lv) <= 1e-4 * abs(lv) + 1e-7, (v, loss[v], lv)
+        b = fwd[v].backward(vp, mode=0)
+        O.densify(b["v_transforms"], b["stats"], b["v_sh"], fwd[v].visible, acc)
+        b64 = oracle_forward(sc, cam, f64=True).backward(vp, mode=0)
+        for k in keys:
+            r32[k] = r32[k] + b[k]
+            r64[k] = r64[k] + b64[k]
+    assert_grad_close(tr.densify.cpu().numpy(), acc, rtol=1e-3, what="densification statistics")
+
+    ctx2 = gsr_ctx_factory(max_splats=sc.n, max_views=nv, max_pixels=64 * 48)
+    sp2 = _dev(sc)
+    ctx2.render_forward(sp2, cams)
+    grads = ctx2.render_backward(sp2, torch.as_tensor(np.concatenate([u.reshape(-1) for u in vps]), device="cuda"))
+    torch.cuda.synchronize()
+    for k in keys:
+        assert_grad_parity(grads[k].cpu().numpy(), r32[k], r64[k], what=k)
+
+
 def test_host_target_pipeline_equals_device_targets(gsr_ctx_factory):
     """train_step_host (targets in pinned host memory, the next step's copy
     prefetched on a side stream while the current step runs) is bit-identical
