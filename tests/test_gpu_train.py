@@ -3,7 +3,7 @@ training step through the C ABI against the CPU oracle."""
 import numpy as np
 import pytest
 
-from _parity import assert_grad_close, oracle_forward, run_gpu_forward
+from _parity import assert_grad_close, oracle_forward, rel_err, run_gpu_forward
 from oracle import oracle as O
 from rustscan_b200 import scenes as S
 
@@ -16,7 +16,7 @@ def _dev(scene):
     return host_splats_to_device(scene)
 
 
-@pytest.mark.parametrize("hw", [(48, 40), (13, 7), (96, 64), (3, 200)])
+@pytest.mark.parametrize("hw", [(48, 40), (13, 7), (96, 64), (3, 200), (1, 1), (1, 37), (37, 1), (2, 2)])
 def test_loss_parity(gsr_ctx_factory, hw):
     import torch
 
@@ -30,7 +30,18 @@ def test_loss_parity(gsr_ctx_factory, hw):
     torch.cuda.synchronize()
     ol, ov = O.loss(pred, tgt)
     assert abs(float(loss[0]) - ol) <= 1e-5 * max(1.0, abs(ol))
-    assert_grad_close(vp.cpu().numpy(), ov, what="d loss / d pred")
+    g = vp.cpu().numpy()
+    _, ov64 = O.loss(pred, tgt, f64=True)
+    own = float(rel_err(ov, ov64).max())
+    if own <= 1e-4:
+        assert_grad_close(g, ov, what="d loss / d pred")
+    else:
+        # A 1x1 image: every blurred moment is the pixel itself, the variance
+        # terms are pure cancellation, and the FP32 oracle's own worst element
+        # is further than 1e-4 from FP64 (2.2e-4). Per element, the GPU must be
+        # no further from FP64 than twice that, plus 1e-4.
+        err = float(rel_err(g, ov64).max())
+        assert err <= 2.0 * own + 1e-4, (err, own)
 
 
 def test_adam_parity(gsr_ctx_factory):
