@@ -64,6 +64,11 @@ constexpr int kBwdPPL16 = 4;
 // One-warp CTA waves (the tile kernel's residency times the SMs) a launch
 // must fill before the 16x16 backward runs one warp per tile.
 constexpr uint32_t kTileKernelWaves = 4;
+// The one-warp backward's batch (entries staged per round, double-buffered)
+// and its resident CTAs per SM: 64 entries take 13 KB of shared memory, so
+// that 16 CTAs fit an SM, the register bound of 16 (at most 128 a thread).
+constexpr int kTileBwdBatch = 64;
+constexpr int kTileBwdBlocks = 16;
 
 struct RasterArgs {
   ViewSet vs;
@@ -977,7 +982,7 @@ __global__ void __launch_bounds__(TW* TH / PPL) raster_bwd_kernel(RasterArgs a) 
 // column share dx and the terms that depend on it; the sigma-gradient
 // moments are kept per column (S1 = dx0 M0_0 + dx1 M0_1 and so on).
 template <int BATCH, bool REF>
-__global__ void __launch_bounds__(32, 16) raster_bwd_tile_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(32, kTileBwdBlocks) raster_bwd_tile_kernel(RasterArgs a) {
   constexpr int NT = 32;
   constexpr int kSI = BATCH / NT;  // entries a lane stages per batch
   static_assert(BATCH % NT == 0, "whole batches per lane");
@@ -1253,7 +1258,7 @@ cudaError_t launch_bwd_mode(const RasterArgs& a, uint32_t batch, int num_sms, cu
 // let 16 CTAs share an SM (a 128-entry batch would fit 9).
 template <bool REF>
 cudaError_t launch_bwd_tile16(const RasterArgs& a, int num_sms, cudaStream_t st) {
-  return launch_items<raster_bwd_tile_kernel<64, REF>>(32, a, num_sms, st);
+  return launch_items<raster_bwd_tile_kernel<kTileBwdBatch, REF>>(32, a, num_sms, st);
 }
 template <int TW, int TH, int PPL>
 cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
@@ -1262,7 +1267,8 @@ cudaError_t launch_bwd_shape(const RasterArgs& a, uint32_t batch, int num_sms, c
 }
 // 16x16 tiles: one warp per tile on large launches, two otherwise.
 cudaError_t launch_bwd_16(const RasterArgs& a, uint32_t batch, int num_sms, cudaStream_t st) {
-  const uint32_t wave = (uint32_t)resident_per_sm<raster_bwd_tile_kernel<64, false>>(32) * (uint32_t)std::max(num_sms, 1);
+  const uint32_t wave =
+      (uint32_t)resident_per_sm<raster_bwd_tile_kernel<kTileBwdBatch, false>>(32) * (uint32_t)std::max(num_sms, 1);
   if (a.vs.total_tiles >= kTileKernelWaves * wave || a.vs.total_tiles == 0)
     return a.ref_mode ? launch_bwd_tile16<true>(a, num_sms, st) : launch_bwd_tile16<false>(a, num_sms, st);
   return launch_bwd_shape<16, 16, kBwdPPL16>(a, batch, num_sms, st);
