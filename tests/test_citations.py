@@ -11,8 +11,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.environ.get("RUSTSCAN_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
-# Files written by the build's reviewers and surveyors, not by this repository.
-SKIP_FILES = {"VERDICT.md", "SURVEY.md", "ADVICE.md", "BASELINE.md"}
+# This repository's own sources and documents (the only files scanned).
+SOURCE_DIRS = ("rustscan_b200", "oracle", "include", "tests")
+SOURCE_FILES = ("bench.py", "__graft_entry__.py", "README.md", "DESIGN.md", "INTEGRATION.md")
 CITE = re.compile(r"((?:[A-Za-z0-9_]+/)*[A-Za-z0-9_]+\.(?:wgsl|rs)):(\d+(?:-\d+)?(?:,\s?\d+(?:-\d+)?)*)")
 
 
@@ -33,12 +34,15 @@ def _resolve(cited, files):
 
 
 def _repo_sources():
-    for dirpath, dirs, names in os.walk(ROOT):
-        dirs[:] = [d for d in dirs if d not in (".git", "_work", "gpurun_out", "_build", "baseline", "__pycache__")]
-        for n in names:
-            if n in SKIP_FILES or not n.endswith((".py", ".cu", ".cuh", ".h", ".cpp", ".md", "Makefile")):
-                continue
-            yield os.path.join(dirpath, n)
+    for f in SOURCE_FILES:
+        if os.path.isfile(os.path.join(ROOT, f)):
+            yield os.path.join(ROOT, f)
+    for top in SOURCE_DIRS:
+        for dirpath, dirs, names in os.walk(os.path.join(ROOT, top)):
+            dirs[:] = [d for d in dirs if d not in ("_build", "__pycache__")]
+            for n in names:
+                if n.endswith((".py", ".cu", ".cuh", ".h", ".cpp", ".md", "Makefile")):
+                    yield os.path.join(dirpath, n)
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "RustGS")), reason="reference checkout not present")

@@ -1,7 +1,8 @@
-"""Uneven multi-view batches in one launch and the autotuner (BASELINE
-config 5 restated at a size the CPU oracle finishes quickly: 30k Gaussians,
-12 views of four resolutions at camera distances U[1.5, 8], so visible
-counts differ about threefold and image sizes 27-fold between views).
+"""Uneven multi-view batches in one launch and the autotuner (the uneven
+batch configuration, config 5, restated at a size the CPU oracle finishes
+quickly: 30k Gaussians, 12 views of four resolutions at camera distances
+U[1.5, 8], so visible counts differ about threefold and image sizes 27-fold
+between views).
 
 Every view of the batch is bit-exact against the oracle's single-view
 forward; the batched backward equals the sum of the per-view oracle

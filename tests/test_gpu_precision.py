@@ -1,4 +1,5 @@
-"""Precision modes through the C ABI (BASELINE config 4 restated at a size
+"""Precision modes through the C ABI (the mixed-precision configuration,
+config 4, restated at a size
 the CPU oracle finishes quickly): BF16 storage of SH coefficients and the
 FP64 2D-covariance inversion for near-degenerate (flattened) Gaussians.
 
