@@ -1,7 +1,7 @@
 """Precision modes through the C ABI (the mixed-precision configuration,
-config 4, restated at a size
-the CPU oracle finishes quickly): BF16 storage of SH coefficients and the
-FP64 2D-covariance inversion for near-degenerate (flattened) Gaussians.
+config 4, restated at a size the CPU oracle finishes quickly): BF16 storage
+of SH coefficients and the FP64 2D-covariance inversion for near-degenerate
+(flattened) Gaussians.
 
 * BF16 storage: the device widens each stored coefficient exactly, so against
   an oracle fed the same BF16-rounded coefficients the forward is bit-exact
