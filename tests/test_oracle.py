@@ -203,12 +203,13 @@ def test_projection_matches_independent_numpy_at_full_size(config):
         assert (np.abs(np.asarray(f.depth, np.float64) - z[gid]) / z[gid]).max() <= tol["z"]
 
 
-def _numpy_tile_counts(m2, con, op, ac, W, H, tw=16, th=16):
+def _numpy_tile_counts(m2, con, op, ac, W, H, tw=16, th=16, pairs=False):
     """Vectorised float64 restatement of the tile box (helpers.wgsl:204-224,
     get_tile_bbox with compute_bbox_extent) and of will_primitive_contribute
     (helpers.wgsl:237-283) for every tile of every box: per Gaussian, the
     passing-tile count and the smallest relative margin |sigma_max - threshold|
-    / max(|threshold|, 1) over its box tiles decided by the sigma test."""
+    / max(|threshold|, 1) over its box tiles decided by the sigma test; with
+    pairs, also the passing (Gaussian, tile id) pairs."""
     pt = np.log(op * 255.0)
     sp = np.maximum(pt, 0.0)
     ex, ey = np.sqrt(np.maximum(0.0, 2 * sp * ac[:, 0])), np.sqrt(np.maximum(0.0, 2 * sp * ac[:, 1]))
@@ -240,7 +241,10 @@ def _numpy_tile_counts(m2, con, op, ac, W, H, tw=16, th=16):
     margin = np.where(inside, np.inf, np.abs(power - pt[g]) / np.maximum(np.abs(pt[g]), 1.0))
     mmin = np.full(len(n), np.inf)
     np.minimum.at(mmin, g, margin)
-    return np.bincount(g, weights=ok, minlength=len(n)).astype(np.int64), mmin
+    counts = np.bincount(g, weights=ok, minlength=len(n)).astype(np.int64)
+    if pairs:
+        return counts, mmin, g[ok], (ty * ntx + tx)[ok]
+    return counts, mmin
 
 
 @pytest.mark.parametrize("config", [2, 3])
@@ -273,6 +277,80 @@ def test_tile_counts_match_independent_numpy_at_full_size(config):
         assert np.abs(diff).max(initial=0) <= 1
         assert len(bad) <= 1e-5 * int(cnt.sum()), len(bad)
         assert (margin[pos[bad]] <= 1e-4).all(), margin[pos[bad]]
+
+
+def _numpy_blend(lt, lg, m2, con, op, rgb, W, H, tw=16, th=16):
+    """Independent float64 restatement of the blend loop (rasterize.wgsl:54-88)
+    for every pixel at once: the per-tile lists (tile ids lt, Gaussians lg,
+    sorted) are walked by rank, each pixel dropping out once its
+    transmittance falls below 1e-4 or its list ends. Returns transmittance,
+    colour (black background), contributor count and last contributor + 1."""
+    ntx, nty = -(-W // tw), -(-H // th)
+    tiles = np.arange(ntx * nty)
+    starts, ends = np.searchsorted(lt, tiles), np.searchsorted(lt, tiles, side="right")
+    ys, xs = np.mgrid[0:H, 0:W]
+    tp = ((ys // th) * ntx + xs // tw).reshape(-1)
+    px, py = xs.reshape(-1) + 0.5, ys.reshape(-1) + 0.5
+    s0, s1 = starts[tp], ends[tp]
+    T, C = np.ones(H * W), np.zeros((H * W, 3))
+    nc, last = np.zeros(H * W, np.int64), np.zeros(H * W, np.int64)
+    active = np.nonzero(s0 < s1)[0]
+    k = 0
+    while active.size:
+        e = s0[active] + k
+        keep = e < s1[active]
+        active, e = active[keep], e[keep]
+        g = lg[e]
+        dx, dy = m2[g, 0] - px[active], m2[g, 1] - py[active]
+        sigma = 0.5 * (con[g, 0] * dx * dx + 2.0 * con[g, 1] * dx * dy + con[g, 2] * dy * dy)
+        alpha = np.minimum(0.999, op[g] * np.exp(-sigma))
+        take = np.nonzero((sigma >= 0) & (alpha >= 1.0 / 255.0))[0]
+        a, at = active[take], alpha[take]
+        C[a] += np.maximum(rgb[g[take]], 0.0) * (at * T[a])[:, None]
+        T[a] *= 1.0 - at
+        nc[a] += 1
+        last[a] = e[take] + 1
+        alive = np.ones(active.size, bool)
+        alive[take[T[a] < 1e-4]] = False
+        active = active[alive]
+        k += 1
+    return T.reshape(H, W), C.reshape(H, W, 3), nc.reshape(H, W), last.reshape(H, W)
+
+
+def test_binning_and_blend_match_independent_numpy_at_full_size():
+    """Config 2 at full size (200,000 Gaussians, 640x480) rebuilt from the
+    float64 restatements alone: the tile lists from the restated tile test
+    ordered by (tile, depth, global id) equal the FP64 oracle's 595,908
+    sorted intersections, and the restated blend over those lists gives the
+    FP64 oracle's contributor counts and last contributors exactly, its
+    transmittance and colour to 1e-12 (colours taken from the oracle's SH
+    evaluation, which is checked against the textbook real SH). The FP32
+    oracle (bit-exact with the GPU) differs in the contributor count of at
+    most 1e-3 of the pixels (decisions FP32 rounding flips; measured 28 of
+    307,200) and by 1e-5 in mean image value (measured 2.8e-7)."""
+    sc = S.config2()
+    cam = sc.cameras[0]
+    vis, m2, con, op, z, ac = _numpy_project_all(sc.transforms, sc.raw_opacity, cam)
+    idx = np.nonzero(vis)[0]
+    _, _, pg, ptile = _numpy_tile_counts(m2[idx], con[idx], op[idx], ac[idx], cam.width, cam.height, pairs=True)
+    gid = idx[pg]
+    order = np.lexsort((gid, z[gid], ptile))
+    lt, lg = ptile[order], gid[order]
+    f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, sc.sh_degree, cam, f64=True)
+    assert np.all(np.asarray(f.bg) == 0)
+    ogid = np.asarray(f.gid)
+    np.testing.assert_array_equal(lt, f.isect_tile.astype(np.int64))
+    np.testing.assert_array_equal(lg, ogid[f.isect_c])
+    rgb = np.zeros((sc.n, 3))
+    rgb[ogid] = np.asarray(f.rec, np.float64)[:, 7:10]
+    T, C, nc, last = _numpy_blend(lt, lg, m2, con, op, rgb, cam.width, cam.height)
+    np.testing.assert_array_equal(nc, f.ncontrib.astype(np.int64))
+    np.testing.assert_array_equal(last, f.last.astype(np.int64))
+    np.testing.assert_allclose(f.tfinal, T, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(f.image[..., :3], C, rtol=0, atol=1e-12)
+    f32 = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, sc.sh_degree, cam)
+    assert int((f32.ncontrib.astype(np.int64) != nc).sum()) <= 1e-3 * nc.size
+    assert float(np.abs(f32.image[..., :3] - C).mean()) <= 1e-5
 
 
 def test_f32_oracle_close_to_f64():
