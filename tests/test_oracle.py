@@ -723,7 +723,7 @@ def _numpy_loss(pred, tgt, l1_weight=0.8, ssim_weight=0.2):
     return l1_weight * np.abs(x - y).mean() + ssim_weight * (1.0 - np.mean(maps))
 
 
-@pytest.mark.parametrize("shape", [(20, 24), (37, 53), (8, 5)])
+@pytest.mark.parametrize("shape", [(20, 24), (37, 53), (8, 5), (1, 1), (1, 37), (720, 1280)])
 def test_loss_value_matches_independent_numpy(shape):
     rng = np.random.default_rng(11)
     H, W = shape
