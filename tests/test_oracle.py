@@ -319,9 +319,10 @@ def _numpy_blend(lt, lg, m2, con, op, rgb, W, H, tw=16, th=16):
 
 def test_binning_and_blend_match_independent_numpy_at_full_size():
     """Config 2 at full size (200,000 Gaussians, 640x480) rebuilt from the
-    float64 restatements alone: the tile lists from the restated tile test
-    ordered by (tile, depth, global id) equal the FP64 oracle's 595,908
-    sorted intersections, and the restated blend over those lists gives the
+    float64 restatements alone: the depth order (ties by global id), the tile
+    lists from the restated tile test ordered by (tile, depth, global id) and
+    their ranges equal the FP64 oracle's (595,908 sorted intersections), and
+    the restated blend over those lists gives the
     FP64 oracle's contributor counts and last contributors exactly, its
     transmittance and colour to 1e-12 (colours taken from the oracle's SH
     evaluation, which is checked against the textbook real SH). The FP32
@@ -341,6 +342,12 @@ def test_binning_and_blend_match_independent_numpy_at_full_size():
     ogid = np.asarray(f.gid)
     np.testing.assert_array_equal(lt, f.isect_tile.astype(np.int64))
     np.testing.assert_array_equal(lg, ogid[f.isect_c])
+    # Depth order (ties by global id) and [start, end) tile ranges.
+    np.testing.assert_array_equal(f.order, np.lexsort((ogid, z[ogid])))
+    tiles = np.arange(f.tiles_x * f.tiles_y)
+    ranges = np.stack([np.searchsorted(lt, tiles), np.searchsorted(lt, tiles, side="right")], -1)
+    ranges[ranges[:, 0] == ranges[:, 1]] = 0  # a tile without intersections keeps (0, 0)
+    np.testing.assert_array_equal(f.ranges.astype(np.int64), ranges.reshape(-1))
     rgb = np.zeros((sc.n, 3))
     rgb[ogid] = np.asarray(f.rec, np.float64)[:, 7:10]
     T, C, nc, last = _numpy_blend(lt, lg, m2, con, op, rgb, cam.width, cam.height)
