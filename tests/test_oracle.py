@@ -804,3 +804,27 @@ def test_sh_colour_matches_standard_real_sh(degree):
         d /= np.linalg.norm(d)
         want = _standard_sh_color(degree, d, sc.sh[g].astype(np.float64))
         np.testing.assert_allclose(f.rec[c, 7:10], want, rtol=1e-12, atol=1e-13)
+
+
+def test_sh_colour_matches_standard_real_sh_at_full_size():
+    """Every visible Gaussian of config 3 view 0 (684,386, SH degree 3): the
+    oracle's colours against the textbook real-SH terms (written out
+    again here, vectorised): FP64 to 1e-13, FP32 (bit-exact with the GPU) to
+    1e-6 absolute."""
+    sc = S.config3()
+    cam = sc.cameras[0]
+    for f64, atol in ((True, 1e-13), (False, 1e-6)):
+        f = O.Forward(sc.transforms, sc.sh, sc.raw_opacity, sc.sh_degree, cam, f64=f64)
+        gid = np.asarray(f.gid)
+        d = sc.transforms[gid, :3].astype(np.float64) - cam.campos.astype(np.float64)
+        x, y, z = (d / np.linalg.norm(d, axis=1, keepdims=True)).T
+        xx, yy, zz = x * x, y * y, z * z
+        basis = [np.full_like(x, 0.28209479177387814), -0.4886025119029199 * y, 0.4886025119029199 * z,
+                 -0.4886025119029199 * x, 1.0925484305920792 * x * y, -1.0925484305920792 * y * z,
+                 0.31539156525252005 * (2 * zz - xx - yy), -1.0925484305920792 * x * z, 0.5462742152960396 * (xx - yy),
+                 -0.5900435899266435 * y * (3 * xx - yy), 2.890611442640554 * x * y * z,
+                 -0.4570457994644658 * y * (4 * zz - xx - yy), 0.3731763325901154 * z * (2 * zz - 3 * xx - 3 * yy),
+                 -0.4570457994644658 * x * (4 * zz - xx - yy), 1.445305721320277 * z * (xx - yy),
+                 -0.5900435899266435 * x * (xx - 3 * yy)]
+        want = np.einsum("kv,vkc->vc", np.asarray(basis), sc.sh[gid].astype(np.float64)) + 0.5
+        np.testing.assert_allclose(np.asarray(f.rec, np.float64)[:, 7:10], want, rtol=0, atol=atol)
