@@ -317,9 +317,11 @@ def _numpy_blend(lt, lg, m2, con, op, rgb, W, H, tw=16, th=16):
     return T.reshape(H, W), C.reshape(H, W, 3), nc.reshape(H, W), last.reshape(H, W)
 
 
-def test_binning_and_blend_match_independent_numpy_at_full_size():
-    """Config 2 at full size (200,000 Gaussians, 640x480) rebuilt from the
-    float64 restatements alone: the depth order (ties by global id), the tile
+@pytest.mark.parametrize("config", [2, 3])
+def test_binning_and_blend_match_independent_numpy_at_full_size(config):
+    """Config 2 (200,000 Gaussians, 640x480) and config 3 view 0 (1,000,000
+    Gaussians, 1280x720, 6,273,270 intersections) at full size, rebuilt from
+    the float64 restatements alone: the depth order (ties by global id), the tile
     lists from the restated tile test ordered by (tile, depth, global id) and
     their ranges equal the FP64 oracle's (595,908 sorted intersections), and
     the restated blend over those lists gives the
@@ -328,8 +330,8 @@ def test_binning_and_blend_match_independent_numpy_at_full_size():
     evaluation, which is checked against the textbook real SH). The FP32
     oracle (bit-exact with the GPU) differs in the contributor count of at
     most 1e-3 of the pixels (decisions FP32 rounding flips; measured 28 of
-    307,200) and by 1e-5 in mean image value (measured 2.8e-7)."""
-    sc = S.config2()
+    307,200 on config 2) and by 1e-5 in mean image value (2.8e-7)."""
+    sc = S.CONFIGS[config]()
     cam = sc.cameras[0]
     vis, m2, con, op, z, ac = _numpy_project_all(sc.transforms, sc.raw_opacity, cam)
     idx = np.nonzero(vis)[0]
