@@ -743,6 +743,32 @@ def test_loss_value_matches_independent_numpy(shape):
         assert abs(val - _numpy_loss(pred, tgt, w1, ws)) <= 1e-12 * max(1.0, abs(val)), (shape, w1, ws)
 
 
+def test_loss_gradient_at_full_size():
+    """The loss gradient on a 1280x720 image pair. SSIM part: against central
+    differences (step 1e-4) of the numpy restatement of the loss along two
+    random directions, 1e-6 relative for the FP64 oracle and 1e-5 for the
+    FP32 one (bit-exact with the GPU's loss kernels' contract). L1 part: the
+    FP64 oracle's gradient is l1_weight / (3 H W) times the sign of x - y,
+    exactly (its kinks make differences along a random direction useless)."""
+    rng = np.random.default_rng(21)
+    H, W = 720, 1280
+    pred = rng.uniform(0, 1, (H, W, 4))
+    tgt = np.clip(pred[..., :3] + rng.normal(0, 0.1, (H, W, 3)), 0, 1)
+    _, g64 = O.loss(pred, tgt, l1_weight=0.0, ssim_weight=1.0, f64=True)
+    _, g32 = O.loss(pred.astype(np.float32), tgt.astype(np.float32), l1_weight=0.0, ssim_weight=1.0)
+    h = 1e-4
+    for _ in range(2):
+        v = rng.standard_normal((H, W, 4))
+        v[..., 3] = 0.0
+        fd = (_numpy_loss(pred + h * v, tgt, 0.0, 1.0) - _numpy_loss(pred - h * v, tgt, 0.0, 1.0)) / (2 * h)
+        d64, d32 = float((g64 * v).sum()), float((g32.astype(np.float64) * v).sum())
+        assert abs(d64 - fd) <= 1e-6 * abs(fd), (d64, fd)
+        assert abs(d32 - fd) <= 1e-5 * abs(fd), (d32, fd)
+    _, gl = O.loss(pred, tgt, l1_weight=0.8, ssim_weight=0.0, f64=True)
+    np.testing.assert_array_equal(gl[..., :3], 0.8 / (3 * H * W) * np.sign(pred[..., :3] - tgt))
+    assert not gl[..., 3].any()
+
+
 @pytest.mark.parametrize("use_visible", [False, True])
 def test_densify_matches_numpy_restatement(use_visible):
     """engine/trainer.rs:651-728 restated in float32 numpy, accumulating into
